@@ -1,0 +1,189 @@
+/*
+ * snc_b200.h -- C ABI of the B200 (sm_100a) execution and training core for
+ * the SNC spiking substrate.
+ *
+ * Plain pointers and sizes only.  Every entry point returns SNC_B200_OK (0) or
+ * a negative snc_b200_status; no C++ exception crosses this boundary.  Unless
+ * a function says "device pointers", every pointer is HOST memory and every
+ * call is synchronous, like the reference's cuda::forward
+ * (src/runtime/cuda_backend.cu:186-361 ends in cudaDeviceSynchronize).
+ *
+ * Reference interfaces this ABI replaces (paths inside blazer502/snc):
+ *   snc::cuda::available / snc::cuda::forward   include/snc/runtime.hpp:61-69
+ *   snc::forward + Backend names                include/snc/runtime.hpp:21-31,57-58
+ *   snc::cudatrain::*                           include/snc/cuda_trainer.hpp:26-57
+ *   python/snc SNN / SurrogateSpike (BPTT)      python/snc/model.py:17-72
+ * INTEGRATION.md shows the bindings a maintainer adds on the reference side.
+ */
+#ifndef SNC_B200_H_
+#define SNC_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SNC_B200_ABI_VERSION 1
+
+typedef enum {
+  SNC_B200_OK = 0,
+  SNC_B200_EINVAL = -1,       /* bad argument or invalid graph */
+  SNC_B200_ENODEV = -2,       /* no usable sm_100 device */
+  SNC_B200_ENOMEM = -3,       /* device allocation failed */
+  SNC_B200_ECUDA = -4,        /* CUDA runtime error (see snc_b200_last_error) */
+  SNC_B200_ETIMEOUT = -5,     /* a bounded device wait gave up */
+  SNC_B200_EUNSUPPORTED = -6, /* graph or config outside this backend's limits */
+  SNC_B200_EOVERFLOW = -7     /* a device work buffer overflowed */
+} snc_b200_status;
+
+/* Read-only view of a reference SNNGraph (include/snc/snn_graph.hpp:114-148):
+ * CSR over OUTGOING synapses, edges in insertion order within each row.
+ * branch_ids is informational in the reference and not needed here. */
+typedef struct {
+  int32_t num_neurons;
+  int32_t num_synapses;
+  const int32_t* row_ptr;  /* [N+1] */
+  const int32_t* post_ids; /* [S] */
+  const float* weights;    /* [S] non-negative efficacy (sign on the pre) */
+  const int32_t* delays;   /* [S] >= 1 */
+  const uint8_t* role;     /* [N] 0 INTERNAL, 1 INPUT, 2 OUTPUT */
+  const int8_t* sign;      /* [N] +1 / -1 */
+  const int32_t* channel;  /* [N] input feature / output class, -1 otherwise */
+} snc_graph_view;
+
+/* InputEvent (include/snc/encoders.hpp:224-229), same 16-byte layout. */
+typedef struct {
+  int32_t sample_id;
+  int32_t channel_id;
+  int32_t time;
+  float amplitude;
+} snc_input_event;
+
+/* LIFParams (include/snc/runtime.hpp:34-39) plus reset_mode:
+ * 0 = v := reset after a spike (the reference), 1 = v := v - threshold. */
+typedef struct {
+  float threshold;
+  float decay;
+  float reset;
+  int32_t refractory;
+  int32_t reset_mode;
+} snc_lif;
+
+/* RunStats (include/snc/runtime.hpp:41-46).  overflow is set on an
+ * SNC_B200_EOVERFLOW return (the reference declares it but never sets it). */
+typedef struct {
+  int64_t spikes;
+  int64_t synaptic_events;
+  int32_t overflow;
+  double ms; /* device time of the step loop (CUDA events) */
+} snc_run_stats;
+
+/* Delivery strategies, the reference's cuda-atomic / cuda-bucket / cuda-sort
+ * (src/runtime/cuda_backend.cu:1-14), re-designed:
+ *   ATOMIC  warp-per-fired-row, coalesced CSR reads, red.add into the ring
+ *   BUCKET  events binned by owning post block, accumulated by that block
+ *   SORT    events applied per ring cell in (step, pre, edge) order: spike
+ *           rasters and membrane potentials bit-identical to the serial CPU
+ *           backend (cpu_backend.cpp:172-181)
+ *   AUTO    chosen per graph by the built-in autotuner (cached per graph) */
+enum {
+  SNC_B200_MODE_ATOMIC = 0,
+  SNC_B200_MODE_BUCKET = 1,
+  SNC_B200_MODE_SORT = 2,
+  SNC_B200_MODE_AUTO = 3
+};
+
+/* Execution paths for a batch of samples. */
+enum {
+  SNC_B200_PATH_PLAIN = 0,      /* per sample, one kernel launch per phase per step */
+  SNC_B200_PATH_PERSISTENT = 1, /* all steps of all samples in one persistent launch */
+  SNC_B200_PATH_AUTO = 2
+};
+
+typedef struct snc_b200_graph snc_b200_graph;   /* device-resident graph */
+typedef struct snc_b200_inputs snc_b200_inputs; /* device-resident input schedule */
+typedef struct snc_b200_run snc_b200_run;       /* device-resident results of one run */
+
+/* ---- device and errors ----------------------------------------------------*/
+
+/* 1 when a usable device of compute capability 10.x is present (replaces
+ * snc::cuda::available, src/runtime/cuda_backend.cu:181-184). */
+int snc_b200_available(void);
+int snc_b200_abi_version(void);
+/* Text of the last error on this host thread ("" if none). */
+const char* snc_b200_last_error(void);
+
+/* ---- graph ----------------------------------------------------------------*/
+
+/* Validate (as SNNGraph::validate, src/graph/snn_graph.cpp:30-56) and upload a
+ * graph once; the reference re-uploads per call (cuda_backend.cu:247-285).
+ * Limits: N < 2^24, max delay <= 255. */
+int snc_b200_graph_upload(const snc_graph_view* g, snc_b200_graph** out);
+int snc_b200_graph_release(snc_b200_graph* g);
+/* Basic shape: N, S, ring length, output channels, input channels. */
+int snc_b200_graph_info(const snc_b200_graph* g, int32_t* n, int32_t* s, int32_t* ring_len,
+                        int32_t* n_out, int32_t* n_in);
+
+/* ---- inputs ----------------------------------------------------------------
+ * Build the per-step injection schedule of a batch of samples on the host
+ * (channel -> INPUT neurons, cpu_backend.cpp:43-65; the drive of one neuron at
+ * one step is summed in event order) and upload it.  events[k].sample_id picks
+ * the sample in [0, num_samples); steps[b] is sample b's step count. */
+int snc_b200_inputs_upload(const snc_b200_graph* g, const snc_input_event* events,
+                           size_t n_events, int32_t num_samples, const int32_t* steps,
+                           snc_b200_inputs** out);
+int snc_b200_inputs_release(snc_b200_inputs* in);
+
+/* ---- run --------------------------------------------------------------------
+ * Run a batch on the device without host synchronisation.  stream is a
+ * cudaStream_t (NULL = the legacy default stream).  flags: */
+enum {
+  SNC_B200_RUN_RASTER = 1, /* keep spike rasters (bit per neuron per step) */
+  SNC_B200_RUN_VFINAL = 2, /* keep final membrane potentials */
+  SNC_B200_RUN_GRAPH = 4,  /* persistent path: launch through a captured CUDA graph */
+  SNC_B200_RUN_FORCE_GRID = 8 /* persistent path: use the all-SM tier even when one
+                                 sample fits in one CTA (tuning and tests) */
+};
+int snc_b200_run_create(const snc_b200_graph* g, const snc_b200_inputs* in, int flags,
+                        snc_b200_run** out);
+int snc_b200_run_release(snc_b200_run* r);
+/* Execute (or re-execute) the run: state is reset, results overwritten. */
+int snc_b200_run_launch(snc_b200_run* r, const snc_lif* lif, int mode, int path, void* stream);
+/* Wait for the run and copy results to host arrays (any may be NULL):
+ *   logits [B][n_out], spikes [B], events [B], raster [sum_b steps[b]][ceil(N/32)]
+ *   (sample-major), v_final [B][N], stats (totals; ms = device time of the
+ *   last launch). */
+int snc_b200_run_fetch(snc_b200_run* r, float* logits, int64_t* spikes, int64_t* events,
+                       uint32_t* raster, float* v_final, snc_run_stats* stats);
+/* The mode and path the last launch actually used (after AUTO resolution). */
+int snc_b200_run_used(const snc_b200_run* r, int* mode, int* path);
+
+/* ---- one-call forward (the reference's cuda::forward, runtime.hpp:66-68) ---
+ * One sample: events are that sample's InputEvents (sample_id ignored);
+ * logits [n_out].  Uses the plain path, like the reference backend.  The
+ * graph is uploaded and released inside the call when `graph` is NULL and
+ * `view` is given; pass an uploaded handle to avoid that. */
+int snc_b200_forward(const snc_b200_graph* graph, const snc_graph_view* view,
+                     const snc_input_event* events, size_t n_events, int32_t num_steps,
+                     const snc_lif* lif, int mode, float* logits, snc_run_stats* stats);
+
+/* Batched forward through the persistent path: many samples with uneven step
+ * counts in one launch.  logits [B][n_out]; spikes / events [B] may be NULL. */
+int snc_b200_forward_batched(const snc_b200_graph* graph, const snc_input_event* events,
+                             size_t n_events, int32_t num_samples, const int32_t* steps,
+                             const snc_lif* lif, int mode, float* logits, int64_t* spikes,
+                             int64_t* events_out, snc_run_stats* stats);
+
+/* ---- delivery autotuner ------------------------------------------------------
+ * Time every (mode, path, block size) candidate on this graph with the given
+ * inputs, cache the winner per graph signature and return it.  Later AUTO
+ * launches on graphs with the same signature reuse the choice. */
+int snc_b200_autotune(const snc_b200_graph* g, const snc_b200_inputs* in, const snc_lif* lif,
+                      int* mode, int* path, int* block_threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SNC_B200_H_ */

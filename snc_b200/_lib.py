@@ -1,0 +1,101 @@
+"""ctypes binding of libsnc_b200.so (the C ABI in include/snc_b200.h).
+
+The library is required: importing a function from here when it is missing
+raises, there is no CPU fallback.  Build it with ``python -m snc_b200.build``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .build import LIB, build, up_to_date
+
+OK, EINVAL, ENODEV, ENOMEM, ECUDA, ETIMEOUT, EUNSUPPORTED, EOVERFLOW = 0, -1, -2, -3, -4, -5, -6, -7
+MODE_ATOMIC, MODE_BUCKET, MODE_SORT, MODE_AUTO = 0, 1, 2, 3
+PATH_PLAIN, PATH_PERSISTENT, PATH_AUTO = 0, 1, 2
+RUN_RASTER, RUN_VFINAL, RUN_GRAPH, RUN_FORCE_GRID = 1, 2, 4, 8
+
+STATUS_NAMES = {0: "OK", -1: "EINVAL", -2: "ENODEV", -3: "ENOMEM", -4: "ECUDA", -5: "ETIMEOUT",
+                -6: "EUNSUPPORTED", -7: "EOVERFLOW"}
+
+
+class SncB200Error(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"snc_b200 {STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class GraphView(C.Structure):
+    _fields_ = [("num_neurons", C.c_int32), ("num_synapses", C.c_int32),
+                ("row_ptr", C.c_void_p), ("post_ids", C.c_void_p), ("weights", C.c_void_p),
+                ("delays", C.c_void_p), ("role", C.c_void_p), ("sign", C.c_void_p),
+                ("channel", C.c_void_p)]
+
+
+class Lif(C.Structure):
+    _fields_ = [("threshold", C.c_float), ("decay", C.c_float), ("reset", C.c_float),
+                ("refractory", C.c_int32), ("reset_mode", C.c_int32)]
+
+
+class RunStats(C.Structure):
+    _fields_ = [("spikes", C.c_int64), ("synaptic_events", C.c_int64), ("overflow", C.c_int32),
+                ("ms", C.c_double)]
+
+
+# name -> (restype, argtypes); every function of include/snc_b200.h
+P = C.c_void_p
+I32 = C.c_int32
+SIGNATURES = {
+    "snc_b200_available": (C.c_int, []),
+    "snc_b200_abi_version": (C.c_int, []),
+    "snc_b200_last_error": (C.c_char_p, []),
+    "snc_b200_graph_upload": (C.c_int, [P, P]),
+    "snc_b200_graph_release": (C.c_int, [P]),
+    "snc_b200_graph_info": (C.c_int, [P, P, P, P, P, P]),
+    "snc_b200_inputs_upload": (C.c_int, [P, P, C.c_size_t, I32, P, P]),
+    "snc_b200_inputs_release": (C.c_int, [P]),
+    "snc_b200_run_create": (C.c_int, [P, P, C.c_int, P]),
+    "snc_b200_run_release": (C.c_int, [P]),
+    "snc_b200_run_launch": (C.c_int, [P, P, C.c_int, C.c_int, P]),
+    "snc_b200_run_fetch": (C.c_int, [P, P, P, P, P, P, P]),
+    "snc_b200_run_used": (C.c_int, [P, P, P]),
+    "snc_b200_forward": (C.c_int, [P, P, P, C.c_size_t, I32, P, C.c_int, P, P]),
+    "snc_b200_forward_batched": (C.c_int, [P, P, C.c_size_t, I32, P, P, C.c_int, P, P, P, P]),
+    "snc_b200_autotune": (C.c_int, [P, P, P, P, P, P]),
+}
+
+_LIB = None
+
+
+def lib():
+    """The loaded library.  Raises when it has not been built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB):
+            raise ImportError(f"{LIB} is missing: build it with `python -m snc_b200.build`")
+        if not up_to_date():
+            build()
+        L = C.CDLL(LIB)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != OK:
+        msg = lib().snc_b200_last_error().decode(errors="replace")
+        raise SncB200Error(rc, f"{what}: {msg}" if what else msg)
+
+
+def ptr(a) -> int | None:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.flags.c_contiguous
+        return a.ctypes.data
+    return a

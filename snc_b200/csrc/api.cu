@@ -1,0 +1,585 @@
+// C ABI implementation: graph upload, input schedules, runs, one-call
+// forwards and the delivery autotuner.  See include/snc_b200.h.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+struct snc_b200_graph : sncb::Graph {};
+struct snc_b200_inputs : sncb::Inputs {};
+struct snc_b200_run : sncb::Run {};
+
+namespace sncb {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int cuda_fail(cudaError_t e, const char* what) {
+  g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+  cudaGetLastError();  // clear a non-sticky error
+  if (e == cudaErrorMemoryAllocation) return SNC_B200_ENOMEM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return SNC_B200_ENODEV;
+  return SNC_B200_ECUDA;
+}
+
+static int check_device() {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    set_error("no CUDA device");
+    return SNC_B200_ENODEV;
+  }
+  int dev = 0, major = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  if (major != 10) {
+    set_error("device is not compute capability 10.x (this library is built for sm_100a)");
+    return SNC_B200_ENODEV;
+  }
+  return SNC_B200_OK;
+}
+
+// SNNGraph::validate (src/graph/snn_graph.cpp:30-56) plus this backend's limits.
+static int validate_view(const snc_graph_view* v) {
+  if (!v) { set_error("null graph"); return SNC_B200_EINVAL; }
+  const int n = v->num_neurons, m = v->num_synapses;
+  if (n < 0 || m < 0) { set_error("negative num_neurons / num_synapses"); return SNC_B200_EINVAL; }
+  if (n > 0 && (!v->row_ptr || !v->role || !v->sign || !v->channel)) {
+    set_error("null per-neuron array"); return SNC_B200_EINVAL;
+  }
+  if (m > 0 && (!v->post_ids || !v->weights || !v->delays)) {
+    set_error("null CSR column array"); return SNC_B200_EINVAL;
+  }
+  if (n > 0 && v->row_ptr[0] != 0) { set_error("row_ptr[0] != 0"); return SNC_B200_EINVAL; }
+  if (n > 0 && v->row_ptr[n] != m) { set_error("row_ptr.back() != num_synapses"); return SNC_B200_EINVAL; }
+  for (int i = 0; i < n; ++i)
+    if (v->row_ptr[i] > v->row_ptr[i + 1]) { set_error("row_ptr not monotone"); return SNC_B200_EINVAL; }
+  for (int s = 0; s < m; ++s) {
+    if (v->post_ids[s] < 0 || v->post_ids[s] >= n) { set_error("post id out of range"); return SNC_B200_EINVAL; }
+    if (v->delays[s] < 1) { set_error("delay < 1"); return SNC_B200_EINVAL; }
+    if (v->delays[s] > 255) { set_error("delay > 255 is outside this backend's limits"); return SNC_B200_EUNSUPPORTED; }
+  }
+  if (n >= (1 << 24)) { set_error("num_neurons >= 2^24 is outside this backend's limits"); return SNC_B200_EUNSUPPORTED; }
+  return SNC_B200_OK;
+}
+
+static void free_graph(Graph* g) {
+  if (!g) return;
+  for (void* p : {(void*)g->row_ptr, (void*)g->edges, (void*)g->post, (void*)g->col_of,
+                  (void*)g->out_ch, (void*)g->role, (void*)g->channel, (void*)g->colbase,
+                  (void*)g->gedges, (void*)g->gptr, (void*)g->groups})
+    dev_free(p);
+}
+
+static int upload_graph(const snc_graph_view* v, Graph* g) {
+  int rc = validate_view(v);
+  if (rc) return rc;
+  const int n = v->num_neurons, m = v->num_synapses;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&g->sm_count, cudaDevAttrMultiProcessorCount, dev);
+  g->N = n;
+  g->S = m;
+  int max_delay = 1;
+  for (int s = 0; s < m; ++s) max_delay = std::max(max_delay, v->delays[s]);
+  g->max_delay = max_delay;
+  g->R = max_delay + 1;
+  // rebuild_io_index (snn_graph.cpp:13-28)
+  int max_in = -1, max_out = -1;
+  for (int i = 0; i < n; ++i) {
+    if (v->role[i] == 1) max_in = std::max(max_in, v->channel[i]);
+    else if (v->role[i] == 2) max_out = std::max(max_out, v->channel[i]);
+  }
+  g->nic = max_in + 1;
+  g->noc = max_out + 1;
+  // channel -> INPUT neurons (ascending id), cpu_backend.cpp:50-55
+  g->chan_ptr_h.assign(std::max(0, g->nic) + 1, 0);
+  for (int i = 0; i < n; ++i)
+    if (v->role[i] == 1 && v->channel[i] >= 0 && v->channel[i] < g->nic) g->chan_ptr_h[v->channel[i] + 1]++;
+  for (int c = 0; c < g->nic; ++c) g->chan_ptr_h[c + 1] += g->chan_ptr_h[c];
+  g->chan_ids_h.assign(g->chan_ptr_h[std::max(0, g->nic)], 0);
+  {
+    std::vector<int> fill(std::max(0, g->nic), 0);
+    for (int i = 0; i < n; ++i)
+      if (v->role[i] == 1 && v->channel[i] >= 0 && v->channel[i] < g->nic)
+        g->chan_ids_h[g->chan_ptr_h[v->channel[i]] + fill[v->channel[i]]++] = i;
+  }
+  // ring columns for neurons with incoming synapses, ascending id
+  std::vector<int> indeg(n, 0);
+  for (int s = 0; s < m; ++s) indeg[v->post_ids[s]]++;
+  g->col_of_h.assign(n, -1);
+  int nc = 0;
+  for (int i = 0; i < n; ++i)
+    if (indeg[i] > 0) g->col_of_h[i] = nc++;
+  g->ncols = nc;
+  std::vector<int> out_ch(n, -1);
+  for (int i = 0; i < n; ++i)
+    if (v->role[i] == 2 && v->channel[i] >= 0) out_ch[i] = v->channel[i];
+  g->row_ptr_h.assign(v->row_ptr, v->row_ptr + n + 1);
+  // packed edges, CSR order (+2 zero entries so 128-bit loads stay in bounds)
+  std::vector<uint2> edges((size_t)m + 2, make_uint2(0, 0));
+  for (int i = 0; i < n; ++i) {
+    const float sg = static_cast<float>(v->sign[i]);
+    for (int e = v->row_ptr[i]; e < v->row_ptr[i + 1]; ++e) {
+      const float w = sg * v->weights[e];
+      uint32_t wb;
+      std::memcpy(&wb, &w, 4);
+      edges[e] = make_uint2((uint32_t)g->col_of_h[v->post_ids[e]] | ((uint32_t)v->delays[e] << 24), wb);
+    }
+  }
+  // block partition for the grid kernels
+  const int sm = std::max(1, g->sm_count);
+  int BS = (n + sm - 1) / sm;
+  BS = std::max(32, (BS + 31) / 32 * 32);
+  const int P = std::max(1, (n + BS - 1) / BS);
+  g->BS = BS;
+  g->P = P;
+  std::vector<int> colbase(P + 1, 0);
+  {
+    int c = 0;
+    for (int b = 0; b < P; ++b) {
+      colbase[b] = c;
+      const int lo = b * BS, hi = std::min(n, lo + BS);
+      for (int j = lo; j < hi; ++j)
+        if (g->col_of_h[j] >= 0) ++c;
+    }
+    colbase[P] = c;
+  }
+  // dest-grouped edges: stable regroup of each row by destination block
+  std::vector<uint2> gedges((size_t)m + 2, make_uint2(0, 0));
+  std::vector<int> gptr(n + 1, 0);
+  std::vector<int2> groups;
+  groups.reserve((size_t)n * 4 + 1);
+  {
+    std::vector<int> idx;
+    for (int i = 0; i < n; ++i) {
+      const int rs = v->row_ptr[i], re = v->row_ptr[i + 1];
+      idx.resize(re - rs);
+      std::iota(idx.begin(), idx.end(), rs);
+      std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+        return v->post_ids[a] / BS < v->post_ids[b] / BS;
+      });
+      int last_blk = -1;
+      for (int q = 0; q < re - rs; ++q) {
+        const int e = idx[q];
+        gedges[rs + q] = edges[e];
+        const int blk = v->post_ids[e] / BS;
+        if (blk != last_blk) {
+          groups.push_back(make_int2(blk, rs + q));
+          last_blk = blk;
+        }
+      }
+      gptr[i + 1] = (int)groups.size();
+    }
+  }
+  // fan-in skew and density for the autotuner signature
+  {
+    double mean = n ? (double)m / n : 0.0, var = 0.0;
+    for (int i = 0; i < n; ++i) var += (indeg[i] - mean) * (indeg[i] - mean);
+    var = n ? var / n : 0.0;
+    g->fanin_cv = mean > 0 ? (float)(std::sqrt(var) / mean) : 0.f;
+    g->density = n > 1 ? (float)((double)m / ((double)n * (n - 1))) : 0.f;
+    const long long lg = (long long)std::log2(std::max(1, n)) * 64 + (long long)std::log2(std::max(1, m));
+    g->signature = (lg << 16) ^ ((long long)(g->fanin_cv * 4) << 8) ^ (long long)g->R;
+  }
+  std::vector<uint8_t> role(v->role, v->role + n);
+  std::vector<int> channel(v->channel, v->channel + n);
+  std::vector<int> post(v->post_ids, v->post_ids + m);
+  if ((rc = dev_upload(&g->row_ptr, v->row_ptr, (size_t)n + 1))) return rc;
+  if ((rc = dev_upload(&g->edges, edges.data(), edges.size()))) return rc;
+  if ((rc = dev_upload(&g->post, post.data(), post.size()))) return rc;
+  if ((rc = dev_upload(&g->col_of, g->col_of_h.data(), (size_t)n))) return rc;
+  if ((rc = dev_upload(&g->out_ch, out_ch.data(), (size_t)n))) return rc;
+  if ((rc = dev_upload(&g->role, role.data(), role.size()))) return rc;
+  if ((rc = dev_upload(&g->channel, channel.data(), channel.size()))) return rc;
+  if ((rc = dev_upload(&g->colbase, colbase.data(), colbase.size()))) return rc;
+  if ((rc = dev_upload(&g->gedges, gedges.data(), gedges.size()))) return rc;
+  if ((rc = dev_upload(&g->gptr, gptr.data(), gptr.size()))) return rc;
+  if ((rc = dev_upload(&g->groups, groups.data(), groups.size()))) return rc;
+  return SNC_B200_OK;
+}
+
+// build_schedule (cpu_backend.cpp:43-65) for a batch: per (sample, step) the
+// (neuron, drive) entries sorted by neuron, each drive summed from 0.0f in
+// event order (cpu_backend.cpp:99).  ignore_sample maps every event to sample 0.
+static int upload_inputs(const Graph* g, const snc_input_event* ev, size_t n_ev, int B,
+                         const int32_t* steps, bool ignore_sample, Inputs* in) {
+  if (B < 0 || (B > 0 && !steps) || (n_ev > 0 && !ev)) {
+    set_error("bad inputs arguments");
+    return SNC_B200_EINVAL;
+  }
+  in->g = g;
+  in->B = B;
+  in->steps_h.assign(steps, steps + B);
+  for (int b = 0; b < B; ++b)
+    if (steps[b] < 0) { set_error("negative step count"); return SNC_B200_EINVAL; }
+  std::vector<long long> stepbase(B + 1, 0);
+  for (int b = 0; b < B; ++b) stepbase[b + 1] = stepbase[b] + steps[b];
+  const long long TS = stepbase[B];
+  in->total_steps = TS;
+  in->Tmax = B ? *std::max_element(steps, steps + B) : 0;
+  const int W = (g->N + 31) / 32;
+  in->raster_off_h.assign(B, 0);
+  for (int b = 0; b < B; ++b) in->raster_off_h[b] = stepbase[b] * W;
+  in->raster_words = TS * W;
+  // bucket by global step, keeping event order
+  std::vector<long long> cnt(TS + 1, 0);
+  auto accept = [&](const snc_input_event& e, int& b) {
+    b = ignore_sample ? 0 : e.sample_id;
+    if (b < 0 || b >= B) return false;
+    if (e.time < 0 || e.time >= steps[b]) return false;
+    if (e.channel_id < 0 || e.channel_id >= g->nic) return false;
+    return true;
+  };
+  for (size_t k = 0; k < n_ev; ++k) {
+    int b;
+    if (!accept(ev[k], b)) continue;
+    cnt[stepbase[b] + ev[k].time + 1] += g->chan_ptr_h[ev[k].channel_id + 1] - g->chan_ptr_h[ev[k].channel_id];
+  }
+  for (long long s = 0; s < TS; ++s) cnt[s + 1] += cnt[s];
+  std::vector<int> nid(cnt[TS]);
+  std::vector<float> amp(cnt[TS]);
+  {
+    std::vector<long long> fill(cnt.begin(), cnt.end() - 1);
+    for (size_t k = 0; k < n_ev; ++k) {
+      int b;
+      if (!accept(ev[k], b)) continue;
+      const long long gs = stepbase[b] + ev[k].time;
+      for (int q = g->chan_ptr_h[ev[k].channel_id]; q < g->chan_ptr_h[ev[k].channel_id + 1]; ++q) {
+        nid[fill[gs]] = g->chan_ids_h[q];
+        amp[fill[gs]] = ev[k].amplitude;
+        ++fill[gs];
+      }
+    }
+  }
+  // per step: stable sort by neuron, then sum duplicates in order
+  std::vector<int> out_nid;
+  std::vector<float> out_ext;
+  out_nid.reserve(nid.size());
+  out_ext.reserve(nid.size());
+  std::vector<int> sptr;
+  sptr.reserve(TS + B);
+  in->sptr_off_h.assign(B, 0);
+  std::vector<int> idx;
+  for (int b = 0; b < B; ++b) {
+    in->sptr_off_h[b] = (long long)sptr.size();
+    for (int t = 0; t < steps[b]; ++t) {
+      sptr.push_back((int)out_nid.size());
+      const long long gs = stepbase[b] + t;
+      const long long k0 = cnt[gs], k1 = cnt[gs + 1];
+      idx.resize(k1 - k0);
+      std::iota(idx.begin(), idx.end(), (int)k0);
+      std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return nid[x] < nid[y]; });
+      for (size_t q = 0; q < idx.size();) {
+        const int id = nid[idx[q]];
+        float acc = 0.0f;
+        while (q < idx.size() && nid[idx[q]] == id) acc += amp[idx[q++]];
+        out_nid.push_back(id);
+        out_ext.push_back(acc);
+      }
+    }
+    sptr.push_back((int)out_nid.size());
+  }
+  if (out_nid.size() > (size_t)INT32_MAX) { set_error("schedule too large"); return SNC_B200_EUNSUPPORTED; }
+  in->n_entries = (long long)out_nid.size();
+  // samples by descending step count (longest first balances uneven lengths)
+  in->order_h.resize(B);
+  std::iota(in->order_h.begin(), in->order_h.end(), 0);
+  std::stable_sort(in->order_h.begin(), in->order_h.end(), [&](int x, int y) { return steps[x] > steps[y]; });
+  int rc;
+  if ((rc = dev_upload(&in->steps, in->steps_h.data(), (size_t)B))) return rc;
+  if ((rc = dev_upload(&in->order, in->order_h.data(), (size_t)B))) return rc;
+  if ((rc = dev_upload(&in->sptr_off, in->sptr_off_h.data(), (size_t)B))) return rc;
+  if ((rc = dev_upload(&in->sched_ptr, sptr.data(), sptr.size()))) return rc;
+  if ((rc = dev_upload(&in->sched_nid, out_nid.data(), out_nid.size()))) return rc;
+  if ((rc = dev_upload(&in->sched_ext, out_ext.data(), out_ext.size()))) return rc;
+  if ((rc = dev_upload(&in->raster_off, in->raster_off_h.data(), (size_t)B))) return rc;
+  return SNC_B200_OK;
+}
+
+static void free_inputs(Inputs* in) {
+  if (!in) return;
+  for (void* p : {(void*)in->steps, (void*)in->order, (void*)in->sptr_off, (void*)in->sched_ptr,
+                  (void*)in->sched_nid, (void*)in->sched_ext, (void*)in->raster_off})
+    dev_free(p);
+}
+
+static void free_run(Run* r) {
+  if (!r) return;
+  if (r->gexec) cudaGraphExecDestroy(r->gexec);
+  for (void* p : {(void*)r->counts, (void*)r->spikes, (void*)r->events, (void*)r->raster,
+                  (void*)r->vfinal, (void*)r->err, (void*)r->ctl, (void*)r->v, (void*)r->refr,
+                  (void*)r->ring, (void*)r->fired, (void*)r->fired_cnt})
+    dev_free(p);
+  if (r->ev0) cudaEventDestroy(r->ev0);
+  if (r->ev1) cudaEventDestroy(r->ev1);
+}
+
+static int create_run(const Graph* g, const Inputs* in, int flags, Run* r) {
+  r->g = g;
+  r->in = in;
+  r->flags = flags;
+  r->W = (g->N + 31) / 32;
+  const size_t B = (size_t)std::max(1, in->B);
+  int rc;
+  if ((rc = dev_alloc(&r->counts, B * std::max(1, g->noc)))) return rc;
+  if ((rc = dev_alloc(&r->spikes, B))) return rc;
+  if ((rc = dev_alloc(&r->events, B))) return rc;
+  if (flags & SNC_B200_RUN_RASTER)
+    if ((rc = dev_alloc(&r->raster, (size_t)std::max<long long>(1, in->raster_words)))) return rc;
+  if (flags & SNC_B200_RUN_VFINAL)
+    if ((rc = dev_alloc(&r->vfinal, B * std::max(1, g->N)))) return rc;
+  if ((rc = dev_alloc(&r->err, 1))) return rc;
+  if ((rc = dev_alloc(&r->ctl, 4))) return rc;
+  SNCB_CUDA(cudaEventCreate(&r->ev0));
+  SNCB_CUDA(cudaEventCreate(&r->ev1));
+  return SNC_B200_OK;
+}
+
+static int fetch_run(Run* r, float* logits, int64_t* spikes, int64_t* events, uint32_t* raster,
+                     float* v_final, snc_run_stats* stats) {
+  const Graph* g = r->g;
+  const Inputs* in = r->in;
+  SNCB_CUDA(cudaEventSynchronize(r->ev1));
+  int err = 0;
+  SNCB_CUDA(cudaMemcpy(&err, r->err, sizeof(int), cudaMemcpyDeviceToHost));
+  float ms = 0.f;
+  SNCB_CUDA(cudaEventElapsedTime(&ms, r->ev0, r->ev1));
+  r->last_ms = ms;
+  const int B = in->B, noc = std::max(1, g->noc);
+  std::vector<int> counts((size_t)std::max(1, B) * noc);
+  std::vector<unsigned long long> sp(std::max(1, B)), evn(std::max(1, B));
+  if (B > 0) {
+    SNCB_CUDA(cudaMemcpy(counts.data(), r->counts, (size_t)B * noc * sizeof(int), cudaMemcpyDeviceToHost));
+    SNCB_CUDA(cudaMemcpy(sp.data(), r->spikes, (size_t)B * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    SNCB_CUDA(cudaMemcpy(evn.data(), r->events, (size_t)B * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  }
+  if (logits)
+    for (int b = 0; b < B; ++b)
+      for (int c = 0; c < g->noc; ++c) logits[(size_t)b * g->noc + c] = (float)counts[(size_t)b * noc + c];
+  long long ts = 0, te = 0;
+  for (int b = 0; b < B; ++b) {
+    if (spikes) spikes[b] = (int64_t)sp[b];
+    if (events) events[b] = (int64_t)evn[b];
+    ts += (long long)sp[b];
+    te += (long long)evn[b];
+  }
+  if (raster) {
+    if (!(r->flags & SNC_B200_RUN_RASTER)) { set_error("run created without SNC_B200_RUN_RASTER"); return SNC_B200_EINVAL; }
+    if (in->raster_words)
+      SNCB_CUDA(cudaMemcpy(raster, r->raster, (size_t)in->raster_words * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  }
+  if (v_final) {
+    if (!(r->flags & SNC_B200_RUN_VFINAL)) { set_error("run created without SNC_B200_RUN_VFINAL"); return SNC_B200_EINVAL; }
+    if (B > 0) SNCB_CUDA(cudaMemcpy(v_final, r->vfinal, (size_t)B * g->N * sizeof(float), cudaMemcpyDeviceToHost));
+  }
+  if (stats) {
+    stats->spikes = ts;
+    stats->synaptic_events = te;
+    stats->overflow = 0;
+    stats->ms = ms;
+  }
+  if (err) {
+    set_error(err == SNC_B200_ETIMEOUT ? "device barrier timed out" : "device error word set");
+    return err < 0 ? err : SNC_B200_ECUDA;
+  }
+  return SNC_B200_OK;
+}
+
+// ---- autotuner --------------------------------------------------------------
+static std::mutex g_tune_mu;
+static std::map<long long, std::pair<int, int>> g_tune_cache;
+
+int resolve_auto(const Graph* g, const Inputs* in, int* mode, int* path) {
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(g->signature);
+    if (it != g_tune_cache.end()) {
+      if (*mode == SNC_B200_MODE_AUTO) *mode = it->second.first;
+      if (*path == SNC_B200_PATH_AUTO) *path = it->second.second;
+      return SNC_B200_OK;
+    }
+  }
+  // untuned default: persistent path; bucketed delivery when the in-degree is
+  // heavily skewed (many sources hammer few targets), atomic otherwise.
+  if (*path == SNC_B200_PATH_AUTO) *path = SNC_B200_PATH_PERSISTENT;
+  if (*mode == SNC_B200_MODE_AUTO) *mode = g->fanin_cv > 1.0f ? SNC_B200_MODE_BUCKET : SNC_B200_MODE_ATOMIC;
+  (void)in;
+  return SNC_B200_OK;
+}
+
+}  // namespace sncb
+
+using namespace sncb;
+
+extern "C" {
+
+int snc_b200_available(void) { return check_device() == SNC_B200_OK ? 1 : 0; }
+
+int snc_b200_abi_version(void) { return SNC_B200_ABI_VERSION; }
+
+const char* snc_b200_last_error(void) { return g_last_error.c_str(); }
+
+int snc_b200_graph_upload(const snc_graph_view* v, snc_b200_graph** out) {
+  if (!out) { set_error("null out"); return SNC_B200_EINVAL; }
+  *out = nullptr;
+  int rc = check_device();
+  if (rc) return rc;
+  auto* g = new snc_b200_graph();
+  rc = upload_graph(v, g);
+  if (rc) { free_graph(g); delete g; return rc; }
+  *out = g;
+  return SNC_B200_OK;
+}
+
+int snc_b200_graph_release(snc_b200_graph* g) {
+  if (!g) return SNC_B200_OK;
+  free_graph(g);
+  delete g;
+  return SNC_B200_OK;
+}
+
+int snc_b200_graph_info(const snc_b200_graph* g, int32_t* n, int32_t* s, int32_t* ring_len,
+                        int32_t* n_out, int32_t* n_in) {
+  if (!g) { set_error("null graph"); return SNC_B200_EINVAL; }
+  if (n) *n = g->N;
+  if (s) *s = g->S;
+  if (ring_len) *ring_len = g->R;
+  if (n_out) *n_out = g->noc;
+  if (n_in) *n_in = g->nic;
+  return SNC_B200_OK;
+}
+
+int snc_b200_inputs_upload(const snc_b200_graph* g, const snc_input_event* events, size_t n_events,
+                           int32_t num_samples, const int32_t* steps, snc_b200_inputs** out) {
+  if (!g || !out) { set_error("null argument"); return SNC_B200_EINVAL; }
+  *out = nullptr;
+  auto* in = new snc_b200_inputs();
+  int rc = upload_inputs(g, events, n_events, num_samples, steps, false, in);
+  if (rc) { free_inputs(in); delete in; return rc; }
+  *out = in;
+  return SNC_B200_OK;
+}
+
+int snc_b200_inputs_release(snc_b200_inputs* in) {
+  if (!in) return SNC_B200_OK;
+  free_inputs(in);
+  delete in;
+  return SNC_B200_OK;
+}
+
+int snc_b200_run_create(const snc_b200_graph* g, const snc_b200_inputs* in, int flags,
+                        snc_b200_run** out) {
+  if (!g || !in || !out || in->g != g) { set_error("bad run arguments"); return SNC_B200_EINVAL; }
+  *out = nullptr;
+  auto* r = new snc_b200_run();
+  int rc = create_run(g, in, flags, r);
+  if (rc) { free_run(r); delete r; return rc; }
+  *out = r;
+  return SNC_B200_OK;
+}
+
+int snc_b200_run_release(snc_b200_run* r) {
+  if (!r) return SNC_B200_OK;
+  free_run(r);
+  delete r;
+  return SNC_B200_OK;
+}
+
+int snc_b200_run_launch(snc_b200_run* r, const snc_lif* lif, int mode, int path, void* stream) {
+  if (!r || !lif) { set_error("null argument"); return SNC_B200_EINVAL; }
+  return launch_run(r, lif, mode, path, static_cast<cudaStream_t>(stream));
+}
+
+int snc_b200_run_fetch(snc_b200_run* r, float* logits, int64_t* spikes, int64_t* events,
+                       uint32_t* raster, float* v_final, snc_run_stats* stats) {
+  if (!r) { set_error("null run"); return SNC_B200_EINVAL; }
+  return fetch_run(r, logits, spikes, events, raster, v_final, stats);
+}
+
+int snc_b200_run_used(const snc_b200_run* r, int* mode, int* path) {
+  if (!r) { set_error("null run"); return SNC_B200_EINVAL; }
+  if (mode) *mode = r->used_mode;
+  if (path) *path = r->used_path;
+  return SNC_B200_OK;
+}
+
+int snc_b200_forward(const snc_b200_graph* graph, const snc_graph_view* view,
+                     const snc_input_event* events, size_t n_events, int32_t num_steps,
+                     const snc_lif* lif, int mode, float* logits, snc_run_stats* stats) {
+  if (!lif) { set_error("null lif"); return SNC_B200_EINVAL; }
+  if (num_steps < 0) { set_error("negative num_steps"); return SNC_B200_EINVAL; }
+  snc_b200_graph* owned = nullptr;
+  int rc;
+  if (!graph) {
+    if ((rc = snc_b200_graph_upload(view, &owned))) return rc;
+    graph = owned;
+  }
+  Inputs in;
+  Run r;
+  rc = upload_inputs(graph, events, n_events, 1, &num_steps, true, &in);
+  if (!rc) rc = create_run(graph, &in, 0, &r);
+  if (!rc) rc = launch_run(&r, lif, mode, SNC_B200_PATH_PLAIN, nullptr);
+  if (!rc) rc = fetch_run(&r, logits, nullptr, nullptr, nullptr, nullptr, stats);
+  free_run(&r);
+  free_inputs(&in);
+  if (owned) snc_b200_graph_release(owned);
+  return rc;
+}
+
+int snc_b200_forward_batched(const snc_b200_graph* graph, const snc_input_event* events,
+                             size_t n_events, int32_t num_samples, const int32_t* steps,
+                             const snc_lif* lif, int mode, float* logits, int64_t* spikes,
+                             int64_t* events_out, snc_run_stats* stats) {
+  if (!graph || !lif) { set_error("null argument"); return SNC_B200_EINVAL; }
+  Inputs in;
+  Run r;
+  int rc = upload_inputs(graph, events, n_events, num_samples, steps, false, &in);
+  if (!rc) rc = create_run(graph, &in, 0, &r);
+  if (!rc) rc = launch_run(&r, lif, mode, SNC_B200_PATH_PERSISTENT, nullptr);
+  if (!rc) rc = fetch_run(&r, logits, spikes, events_out, nullptr, nullptr, stats);
+  free_run(&r);
+  free_inputs(&in);
+  return rc;
+}
+
+int snc_b200_autotune(const snc_b200_graph* g, const snc_b200_inputs* in, const snc_lif* lif,
+                      int* mode, int* path, int* block_threads) {
+  if (!g || !in || !lif) { set_error("null argument"); return SNC_B200_EINVAL; }
+  Run r;
+  int rc = create_run(g, in, 0, &r);
+  if (rc) { free_run(&r); return rc; }
+  float best = 1e30f;
+  int bm = SNC_B200_MODE_ATOMIC, bp = SNC_B200_PATH_PERSISTENT;
+  for (int p = SNC_B200_PATH_PLAIN; p <= SNC_B200_PATH_PERSISTENT; ++p)
+    for (int m = SNC_B200_MODE_ATOMIC; m <= SNC_B200_MODE_SORT; ++m) {
+      float t = 0.f;
+      for (int rep = 0; rep < 2; ++rep) {  // first launch warms up
+        rc = launch_run(&r, lif, m, p, nullptr);
+        if (!rc) rc = fetch_run(&r, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+        if (rc) break;
+        t = r.last_ms;
+      }
+      if (rc) { free_run(&r); return rc; }
+      if (t < best) { best = t; bm = m; bp = p; }
+    }
+  free_run(&r);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[g->signature] = {bm, bp};
+  }
+  if (mode) *mode = bm;
+  if (path) *path = bp;
+  if (block_threads) *block_threads = bp == SNC_B200_PATH_PERSISTENT && g->N <= 8192 ? 1024 : 512;
+  return SNC_B200_OK;
+}
+
+}  // extern "C"

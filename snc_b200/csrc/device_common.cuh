@@ -1,0 +1,184 @@
+// Device helpers shared by the forward, e-prop and BPTT kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sncb {
+
+// Wall-clock bound of every spin-wait in this library: a wait that has not
+// finished after this many nanoseconds sets the error word and returns.
+constexpr unsigned long long kSpinTimeoutNs = 2000000000ull;  // 2 s
+constexpr int kErrTimeout = -5;                               // SNC_B200_ETIMEOUT
+
+struct LifP {
+  float thr, decay, reset;
+  int refractory, reset_mode;
+};
+
+// cpu_backend.cpp:134 -- v * decay + ext + slot as three separately rounded
+// IEEE operations in the CPU's order (no fused multiply-add), so the GPU and
+// the serial CPU backend produce identical bits from identical inputs.
+__device__ __forceinline__ float lif_integrate(float v, float decay, float ext, float ring) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(v, decay), ext), ring);
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ int ld_volatile_i32(const int* p) {
+  return *reinterpret_cast<const volatile int*>(p);
+}
+
+__device__ __forceinline__ void red_release_add_u32(unsigned* p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Block-wide exclusive scan of one int per thread (blockDim a multiple of 32,
+// at most 1024).  scratch: >= 33 ints of shared memory.  Returns this
+// thread's exclusive prefix and writes the block total to *total.
+__device__ __forceinline__ int block_exclusive_scan(int x, int* scratch, int* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  int incl = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) scratch[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int s = lane < nw ? scratch[lane] : 0;
+    int si = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, si, o);
+      if (lane >= o) si += y;
+    }
+    if (lane < nw) scratch[lane] = si - s;
+    if (lane == 31) scratch[32] = si;
+  }
+  __syncthreads();
+  const int res = scratch[warp] + incl - x;
+  *total = scratch[32];
+  __syncthreads();
+  return res;
+}
+
+// Block-wide sum of one 64-bit value per thread; result valid in all threads.
+__device__ __forceinline__ long long block_sum_ll(long long x, long long* scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+  if (lane == 0) scratch[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    long long s = lane < nw ? scratch[lane] : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) scratch[32] = s;
+  }
+  __syncthreads();
+  const long long r = scratch[32];
+  __syncthreads();
+  return r;
+}
+
+// Software grid barrier for a cooperatively launched (co-resident) grid.
+// `ctr` counts arrivals and is never reset inside a launch; the n-th barrier
+// of the launch waits for ctr >= n * gridDim.x.  The wait is bounded: after
+// kSpinTimeoutNs it records kErrTimeout in *err and every CTA returns false,
+// so callers leave their loops and the context stays usable.
+__device__ __forceinline__ bool grid_sync(unsigned* ctr, unsigned target, int* err) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    red_release_add_u32(ctr, 1u);
+    int ok = 1;
+    const unsigned long long t0 = global_ns();
+    unsigned spins = 0;
+    while (ld_acquire_u32(ctr) < target) {
+      if (ld_volatile_i32(err) != 0) { ok = 0; break; }
+      if ((++spins & 63u) == 0 && global_ns() - t0 > kSpinTimeoutNs) {
+        atomicCAS(err, 0, kErrTimeout);
+        ok = 0;
+        break;
+      }
+      __nanosleep(20);
+    }
+    __threadfence();
+    s_ok = ok && ld_volatile_i32(err) == 0;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Largest k in [0, n) with a[k] <= x, for a non-decreasing a with a[0] <= x.
+__device__ __forceinline__ int upper_index(const int* a, int n, int x) {
+  int lo = 0, hi = n;  // invariant: a[lo] <= x, answer in [lo, hi)
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (a[mid] <= x) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// First k in [lo, hi) with a[k] >= x (hi when none).
+__device__ __forceinline__ int lower_bound_i(const int* a, int lo, int hi, int x) {
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (a[mid] < x) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// Edge packing: x = ring column (24 bits) | delay << 24, y = signed weight bits.
+__device__ __forceinline__ int edge_col(uint2 e) { return static_cast<int>(e.x & 0xFFFFFFu); }
+__device__ __forceinline__ int edge_delay(uint2 e) { return static_cast<int>(e.x >> 24); }
+__device__ __forceinline__ float edge_w(uint2 e) { return __uint_as_float(e.y); }
+
+}  // namespace sncb
+
+namespace sncb {
+
+// Ordered compaction of one flag per thread with warp ballot / popc: returns
+// the number of flagged threads before this one in thread order, writes the
+// block total to *total and this warp's ballot to *mask.  scratch >= 33 ints.
+__device__ __forceinline__ int ballot_compact(int flag, int* scratch, int* total, unsigned* mask) {
+  const unsigned m = __ballot_sync(0xffffffffu, flag);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  if (lane == 0) scratch[warp] = __popc(m);
+  __syncthreads();
+  if (warp == 0) {
+    const int c = lane < nw ? scratch[lane] : 0;
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane < nw) scratch[lane] = incl - c;
+    if (lane == 31) scratch[32] = incl;
+  }
+  __syncthreads();
+  const int pos = scratch[warp] + __popc(m & ((1u << lane) - 1u));
+  *total = scratch[32];
+  *mask = m;
+  __syncthreads();
+  return pos;
+}
+
+}  // namespace sncb

@@ -1,0 +1,127 @@
+// Host-side structures shared by the C ABI implementation files.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/snc_b200.h"
+
+namespace sncb {
+
+void set_error(const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);  // records and maps to a status
+
+#define SNCB_CUDA(call)                                  \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+  } while (0)
+
+template <typename T>
+int dev_upload(T** d, const T* h, size_t n) {
+  *d = nullptr;
+  if (n == 0) n = 1;
+  SNCB_CUDA(cudaMalloc(reinterpret_cast<void**>(d), n * sizeof(T)));
+  if (h) SNCB_CUDA(cudaMemcpy(*d, h, n * sizeof(T), cudaMemcpyHostToDevice));
+  return SNC_B200_OK;
+}
+
+template <typename T>
+int dev_alloc(T** d, size_t n) {
+  *d = nullptr;
+  if (n == 0) n = 1;
+  SNCB_CUDA(cudaMalloc(reinterpret_cast<void**>(d), n * sizeof(T)));
+  return SNC_B200_OK;
+}
+
+inline void dev_free(void* p) {
+  if (p) cudaFree(p);
+}
+
+// Device-resident graph.  Neurons with at least one incoming synapse own a
+// ring column (col_of[j] >= 0, assigned in ascending id order); the delay
+// ring of one sample is [ring_len][ncols] floats.  Edges are packed 8 bytes:
+// x = ring column of the post | delay << 24, y = sign[pre] * weight.
+struct Graph {
+  int N = 0, S = 0, R = 0, ncols = 0, noc = 0, nic = 0, max_delay = 1;
+  int sm_count = 0;
+  // host copies used by the schedule builder and the adapters
+  std::vector<int> row_ptr_h, chan_ptr_h, chan_ids_h, col_of_h;
+  // device, CSR (insertion) order
+  int* row_ptr = nullptr;   // [N+1]
+  uint2* edges = nullptr;   // [S]
+  int* post = nullptr;      // [S] post neuron ids (e-prop update)
+  int* col_of = nullptr;    // [N]
+  int* out_ch = nullptr;    // [N] output channel or -1
+  uint8_t* role = nullptr;  // [N]
+  int* channel = nullptr;   // [N]
+  // block partition for the multi-CTA (grid) kernels: block b owns neurons
+  // [b*BS, min(N,(b+1)*BS)) and their ring columns [colbase[b], colbase[b+1]).
+  int P = 0, BS = 0;
+  int* colbase = nullptr;   // [P+1]
+  // dest-grouped edges: each row's edges stably regrouped by destination
+  // block; group g of row i is (block, first edge) for g in [gptr[i], gptr[i+1]).
+  uint2* gedges = nullptr;  // [S]
+  int* gptr = nullptr;      // [N+1]
+  int2* groups = nullptr;   // [G]
+  long long signature = 0;  // autotuner cache key
+  float fanin_cv = 0.f, density = 0.f;
+};
+
+struct Inputs {
+  const Graph* g = nullptr;
+  int B = 0, Tmax = 0;
+  long long total_steps = 0, raster_words = 0;
+  std::vector<int> steps_h, order_h;
+  std::vector<long long> sptr_off_h, raster_off_h;
+  int* steps = nullptr;         // [B]
+  int* order = nullptr;         // [B] samples by descending step count
+  long long* sptr_off = nullptr;  // [B] start of sample b's step pointers
+  int* sched_ptr = nullptr;     // concatenated [T_b + 1] absolute entry offsets
+  int* sched_nid = nullptr;     // entries sorted by neuron within a step
+  float* sched_ext = nullptr;   // drive summed in event order
+  long long* raster_off = nullptr;  // [B] first raster word of sample b
+  long long n_entries = 0;
+};
+
+struct Run {
+  const Graph* g = nullptr;
+  const Inputs* in = nullptr;
+  int flags = 0;
+  int W = 0;  // raster words per step
+  // outputs
+  int* counts = nullptr;                 // [B][noc]
+  unsigned long long* spikes = nullptr;  // [B]
+  unsigned long long* events = nullptr;  // [B]
+  uint32_t* raster = nullptr;            // [raster_words]
+  float* vfinal = nullptr;               // [B][N]
+  // control
+  int* err = nullptr;
+  unsigned* ctl = nullptr;  // [0] barrier counter, [1] work-queue counter
+  // grid-path state (one wave of Bw samples in lockstep)
+  int Bw = 0;
+  float* v = nullptr;
+  int* refr = nullptr;
+  float* ring = nullptr;
+  int* fired = nullptr;      // [Bw][2][N]
+  int* fired_cnt = nullptr;  // [Bw][2][P]
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+  int used_mode = -1, used_path = -1;
+  // captured launch of the persistent path
+  cudaGraphExec_t gexec = nullptr;
+  int gexec_mode = -1;
+  snc_lif gexec_lif{};
+  cudaStream_t gexec_stream = nullptr;
+};
+
+// forward.cu
+int launch_run(Run* r, const snc_lif* lif, int mode, int path, cudaStream_t stream);
+int tier_s_smem_bytes(const Graph* g, int mode, bool eprop);
+int resolve_auto(const Graph* g, const Inputs* in, int* mode, int* path);
+
+}  // namespace sncb

@@ -1,0 +1,159 @@
+"""Parity of the B200 forward kernels against the CPU oracle and the
+reference fixtures, through the C ABI.
+
+SORT delivery must reproduce the serial CPU backend bit for bit: spike
+rasters, final membrane potentials, logits, spike and event counts.  ATOMIC
+and BUCKET delivery reorder float additions, so they are held to total
+spike-count agreement >= 99.9% (the north-star tolerance for atomic mode).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from snc_b200 import runtime as R
+from snc_b200 import workloads as W
+from tests.helpers import golden, spike_count_agreement, to_lif
+
+pytestmark = pytest.mark.gpu
+
+PATHS = [("plain", R.PATH_PLAIN, False), ("tierS", R.PATH_PERSISTENT, False),
+         ("tierG", R.PATH_PERSISTENT, True)]
+
+
+def run_gpu(g, ev, steps, lif, mode, path, force_grid=False, cuda_graph=False, repeat=1):
+    dg = R.DeviceGraph(g)
+    di = R.DeviceInputs(dg, ev, steps)
+    run = R.Run(dg, di, raster=True, vfinal=True, cuda_graph=cuda_graph, force_grid=force_grid)
+    for _ in range(repeat):
+        run.launch(lif, mode=mode, path=path)
+        out = run.fetch(raster=True, vfinal=True)
+    out["used"] = run.used()
+    return out
+
+
+def assert_exact(out, ref):
+    np.testing.assert_array_equal(out["spikes"], ref["spikes"])
+    np.testing.assert_array_equal(out["events"], ref["events"])
+    np.testing.assert_array_equal(out["logits"], ref["logits"])
+    np.testing.assert_array_equal(out["raster"], ref["raster"])
+    np.testing.assert_array_equal(out["v"].view(np.uint32), ref["v"].view(np.uint32))
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+@pytest.mark.parametrize("lifcfg", [(0, 1), (1, 0), (0, 2)])
+@pytest.mark.parametrize("pname,path,force", PATHS)
+def test_sort_bit_exact_random(seed, lifcfg, pname, path, force):
+    reset_mode, refractory = lifcfg
+    g = W.random_graph(seed, max_delay=2 + seed * 3)
+    ev, steps = W.random_events(seed + 10, g, 4, [37, 5, 60, 0])
+    lif = R.LIFParams(threshold=1.0, decay=0.9, reset=0.0, refractory=refractory,
+                      reset_mode=reset_mode)
+    ref = O.forward_batched(g, ev, steps, lif)
+    out = run_gpu(g, ev, steps, lif, R.MODE_SORT, path, force_grid=force)
+    assert_exact(out, ref)
+
+
+@pytest.mark.parametrize("mode", [R.MODE_ATOMIC, R.MODE_BUCKET])
+@pytest.mark.parametrize("pname,path,force", PATHS)
+def test_unordered_modes_spike_agreement(mode, pname, path, force):
+    g = W.random_graph(5, n_hid=200, max_delay=6)
+    ev, steps = W.random_events(9, g, 6, 80)
+    lif = R.LIFParams(threshold=1.0, decay=0.9, refractory=1)
+    ref = O.forward_batched(g, ev, steps, lif)
+    out = run_gpu(g, ev, steps, lif, mode, path, force_grid=force)
+    assert spike_count_agreement(out["spikes"], ref["spikes"]) >= 0.999
+    assert out["used"] == (mode, path)
+
+
+@pytest.mark.parametrize("prefix", ["static", "rsparse", "sdelay"])
+@pytest.mark.parametrize("pname,path,force", PATHS)
+def test_reference_fixture(prefix, pname, path, force):
+    """Outputs of the unchanged reference CPU backend (tests/golden)."""
+    g, ev, steps, lifns, exp = golden(prefix)
+    lif = to_lif(lifns)
+    out = run_gpu(g, ev, steps, lif, R.MODE_SORT, path, force_grid=force)
+    np.testing.assert_array_equal(out["spikes"], exp["spikes"])
+    np.testing.assert_array_equal(out["events"], exp["events"])
+    np.testing.assert_array_equal(out["logits"], exp["logits"])
+
+
+def test_one_call_forward_matches_reference_fixture():
+    """snc_b200_forward: the cuda::forward replacement (graph uploaded inside)."""
+    g, ev, steps, lifns, exp = golden("static")
+    lif = to_lif(lifns)
+    for i in range(3):
+        evi = ev[ev["sample_id"] == i]
+        r = R.forward(g, evi, int(steps[i]), lif, backend="cuda-sort")
+        np.testing.assert_array_equal(r.logits, exp["logits"][i])
+        assert r.stats.spikes == exp["spikes"][i]
+        assert r.stats.synaptic_events == exp["events"][i]
+        assert r.used_backend == "b200-sort"
+
+
+def test_ff784_persistent_vs_oracle():
+    g = W.ff784_graph()
+    ev, steps = W.ff784_inputs(64)
+    lif = W.lif_tau20()
+    ref = O.forward_batched(g, ev, steps, lif)
+    out = run_gpu(g, ev, steps, lif, R.MODE_SORT, R.PATH_PERSISTENT, cuda_graph=True, repeat=2)
+    assert_exact(out, ref)
+
+
+def test_audio700_uneven_persistent_vs_oracle():
+    g = W.audio700_graph()
+    ev, steps = W.audio700_inputs(12)
+    lif = W.lif_tau20()
+    ref = O.forward_batched(g, ev, steps, lif)
+    for force in (False, True):
+        out = run_gpu(g, ev, steps, lif, R.MODE_SORT, R.PATH_PERSISTENT, force_grid=force)
+        assert_exact(out, ref)
+
+
+@pytest.fixture(scope="module")
+def rec100k():
+    g = W.rec100k_graph()
+    ev, steps = W.rec100k_inputs(g, num_samples=2, num_steps=300)
+    lif = W.lif_tau20()
+    return g, ev, steps, lif, O.forward_batched(g, ev, steps, lif)
+
+
+@pytest.mark.parametrize("path", [R.PATH_PLAIN, R.PATH_PERSISTENT])
+def test_rec100k_sort_bit_exact(rec100k, path):
+    g, ev, steps, lif, ref = rec100k
+    out = run_gpu(g, ev, steps, lif, R.MODE_SORT, path, cuda_graph=(path == R.PATH_PERSISTENT))
+    assert_exact(out, ref)
+
+
+@pytest.mark.parametrize("mode", [R.MODE_ATOMIC, R.MODE_BUCKET])
+def test_rec100k_unordered(rec100k, mode):
+    g, ev, steps, lif, ref = rec100k
+    out = run_gpu(g, ev, steps, lif, mode, R.PATH_PERSISTENT)
+    assert spike_count_agreement(out["spikes"], ref["spikes"]) >= 0.999
+    np.testing.assert_array_equal(out["events"].sum() > 0, True)
+
+
+def test_empty_and_zero_step_inputs():
+    g = W.random_graph(4)
+    lif = R.LIFParams()
+    out = run_gpu(g, None, [0, 3, 0], lif, R.MODE_SORT, R.PATH_PERSISTENT)
+    ref = O.forward_batched(g, np.zeros(0, dtype=O.EVENT_DTYPE), [0, 3, 0], lif)
+    assert_exact(out, ref)
+    assert out["spikes"].sum() == 0
+
+
+def test_batched_one_call_and_autotune():
+    g = W.random_graph(6, n_hid=120)
+    ev, steps = W.random_events(3, g, 5, [30, 40, 50, 20, 10])
+    lif = R.LIFParams(refractory=1)
+    ref = O.forward_batched(g, ev, steps, lif)
+    dg = R.DeviceGraph(g)
+    out = R.forward_batched(dg, ev, steps, lif, mode=R.MODE_SORT)
+    np.testing.assert_array_equal(out["spikes"], ref["spikes"])
+    np.testing.assert_array_equal(out["logits"], ref["logits"])
+    di = R.DeviceInputs(dg, ev, steps)
+    best = R.autotune(dg, di, lif)
+    assert best["mode"] in (0, 1, 2) and best["path"] in (0, 1)
+    run = R.Run(dg, di)
+    run.launch(lif, mode=R.MODE_AUTO, path=R.PATH_AUTO)
+    run.fetch()
+    assert run.used() == (best["mode"], best["path"])
