@@ -1,0 +1,337 @@
+#!/usr/bin/env python
+"""Benchmark of the spiking substrate's forward hot path on B200.
+
+Workload (one "step" = one full forward of it): rec100k, the large recurrent
+substrate -- 100k LIF neurons on a 2-D torus, 10M synapses (95 local targets
+with lognormal in-degree skew + 5 long-range per neuron), delays 1-30, 10% of
+neurons Poisson-driven at 0.02 spikes/step, 1000 timesteps, batch 1.  Seeded
+synthetic graph and inputs (snc_b200/workloads.py).
+
+Our arm (default): the batched persistent path (one launch for all 1000
+timesteps, CUDA-graph captured) in the delivery mode the autotuner picks.
+  value  synaptic events/s, inputs and graph resident in HBM, L2 flushed
+         (256 MiB write) before every timed step, CUDA-event device time.
+  e2e    the same metric through snc_b200_forward_batched with host event
+         arrays: schedule build, host->device copy, run and result read-back
+         inside the timed region (wall clock).
+Extra keys report sample-steps/s, the plain per-sample path, the
+bit-identical SORT mode and the ratio persistent / plain.
+
+Reference arm (--impl reference): the reference's own CPU backend (compiled
+from its sources into oracle/_ref, snc::forward with the OpenMP backend, all
+host threads) on the same workload; rank 0 only.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("synaptic events/s and sample-steps/s, batched vs plain path, 1 B200; BPTT step ms")
+UNIT = "synaptic events/s"
+WORKLOAD = "rec100k: 100k LIF, 10M synapses, delays 1-30, 1000 steps, batch 1"
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=40)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--mode", default="auto", choices=["auto", "atomic", "bucket", "sort"])
+    p.add_argument("--no-extra", action="store_true", help="skip the plain / sort / cpu legs")
+    return p.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def alg_bytes(events, spikes, neuron_steps):
+    """Algorithmic bytes of one forward: 12 B per synaptic event (post id,
+    weight, delay), 8 B per spike (row bounds), 32 B per neuron-step
+    (v, refr, drive, ring slot: read + write)."""
+    return 12 * events + 8 * spikes + 32 * neuron_steps
+
+
+class Clocks:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "50", "-i", str(self.gpu_id)],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = float(f[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def reference_arm(args):
+    rank, world, _ = dist_setup()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    from snc_b200 import workloads as W
+    g = W.rec100k_graph(seed=1)
+    ev, steps = W.rec100k_inputs(g, 1, 1000, seed=1)
+    lif = W.lif_tau20()
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    if O.ref_available():
+        kind = "reference"
+        rg = O.RefGraph(g)
+        fwd = lambda: rg.forward(ev, 1000, lif, backend="openmp")  # noqa: E731
+    else:
+        kind, threads = "port", 1
+        fwd = lambda: O.forward(g, ev, 1000, lif)  # noqa: E731
+    for _ in range(args.warmup):
+        fwd()
+    t_tot, e_tot = 0.0, 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r = fwd()
+        t_tot += time.perf_counter() - t0
+        e_tot += r["events"]
+    value = e_tot / t_tot
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_tot / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "backend": "openmp" if kind == "reference" else "serial"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": "full rec100k forward (1000 steps, batch 1) per step"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline(g, ev, lif, budget_s=10.0):
+    """The reference CPU backend (serial), timed on this host on whole
+    rec100k samples until ~budget_s of work."""
+    from oracle import oracle as O
+    if O.ref_available():
+        kind = "reference"
+        rg = O.RefGraph(g)
+        fwd = lambda: rg.forward(ev, 1000, lif, backend="cpu")  # noqa: E731
+    else:
+        kind = "port"
+        fwd = lambda: O.forward(g, ev, 1000, lif)  # noqa: E731
+    n, t, e = 0, 0.0, 0
+    while t < budget_s or n < 2:
+        t0 = time.perf_counter()
+        r = fwd()
+        t += time.perf_counter() - t0
+        e += r["events"]
+        n += 1
+    return {"value": e / t, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"{n} full rec100k forwards (1000 steps, batch 1), serial cpu backend"}
+
+
+def our_arm(args):
+    import torch
+    rank, world, local = dist_setup()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    from snc_b200 import runtime as R
+    from snc_b200 import workloads as W
+    R.set_device(local)
+    lif = W.lif_tau20()
+    g = W.rec100k_graph(seed=1)
+    ev, steps = W.rec100k_inputs(g, 1, 1000, seed=1 + rank)
+    dg = R.DeviceGraph(g)
+    di = R.DeviceInputs(dg, ev, steps)
+    modes = {"atomic": R.MODE_ATOMIC, "bucket": R.MODE_BUCKET, "sort": R.MODE_SORT}
+    if args.mode == "auto":
+        tuned = R.autotune(dg, di, lif)
+        mode = tuned["mode"] if tuned["path"] == R.PATH_PERSISTENT else R.MODE_BUCKET
+    else:
+        mode = modes[args.mode]
+    run = R.Run(dg, di, cuda_graph=True)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def timed(run_, mode_, path_, k):
+        ms, ev_n, sp_n = [], 0, 0
+        for _ in range(k):
+            flush.zero_()
+            run_.launch(lif, mode=mode_, path=path_)
+            o = run_.fetch()
+            ms.append(o["ms"])
+            ev_n += o["total_events"]
+            sp_n += o["total_spikes"]
+        return ms, ev_n, sp_n
+
+    timed(run, mode, R.PATH_PERSISTENT, args.warmup)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    dev_props = torch.cuda.get_device_properties(local)
+    clocks = Clocks(f"GPU-{dev_props.uuid}" if getattr(dev_props, "uuid", None) else local)
+    clocks.start()
+    ms, ev_n, sp_n = timed(run, mode, R.PATH_PERSISTENT, args.steps)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    used_graph = run.used_graph()
+    tot_ms = float(sum(ms))
+    if dist:
+        t = torch.tensor([tot_ms, float(ev_n)], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        tot_ms_max, ev_all = float(mx[0]), float(t[1])
+    else:
+        tot_ms_max, ev_all = tot_ms, float(ev_n)
+    value = ev_all / (tot_ms_max / 1e3)
+    ms_per_step = tot_ms_max / args.steps
+
+    # end to end through the C ABI with host buffers
+    e2e_t, e2e_ev = 0.0, 0
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        o = R.forward_batched(dg, ev, steps, lif, mode=mode)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e_t += dt
+            e2e_ev += int(o["events"].sum())
+    if dist:
+        t = torch.tensor([e2e_t, float(e2e_ev)], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        e2e_t, e2e_ev = float(mx[0]), float(t[1])
+    e2e = {"value": e2e_ev / e2e_t, "unit": UNIT, "h2d_bytes_per_step": int(di.device_bytes),
+           "d2h_bytes_per_step": int(4 * max(1, dg.n_out) + 16 + 4)}
+
+    extra = {}
+    if not args.no_extra:
+        k2 = max(2, min(5, args.steps))
+        for name, m, p in (("plain_sort", R.MODE_SORT, R.PATH_PLAIN),
+                           ("persistent_sort", R.MODE_SORT, R.PATH_PERSISTENT),
+                           ("plain_best", mode, R.PATH_PLAIN)):
+            r2 = R.Run(dg, di, cuda_graph=(p == R.PATH_PERSISTENT))
+            timed(r2, m, p, 1)
+            ms2, ev2, _ = timed(r2, m, p, k2)
+            extra[name] = {"events_per_s": ev2 / (sum(ms2) / 1e3), "ms_per_step": sum(ms2) / k2,
+                           "mode": R.MODE_NAMES[m]}
+            r2.release()
+        extra["persistent_vs_plain_sort"] = extra["persistent_sort"]["events_per_s"] / extra["plain_sort"]["events_per_s"]
+
+    peak, peak_kind = peaks()
+    per_launch_bytes = alg_bytes(ev_n / args.steps, sp_n / args.steps, g.num_neurons * 1000)
+    achieved = per_launch_bytes / (tot_ms / args.steps / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "rec100k_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            with open(tpath) as f:
+                traffic = json.load(f).get(R.MODE_NAMES[mode])
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                "kernel": "k_tier_g", "bytes_per_launch": per_launch_bytes}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_extra:
+        cpu = cpu_baseline(g, ev, lif)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded graph and Poisson drive, snc_b200/workloads.py)",
+                "config": {"workload": WORKLOAD, "path": "persistent", "mode": R.MODE_NAMES[mode],
+                           "cuda_graph": used_graph, "l2": "flushed (256 MiB write) before each timed step",
+                           "parallelism": f"replicas x{world}" if world > 1 else "single"},
+                "sample_steps_per_s": world * 1000 * args.steps / (tot_ms_max / 1e3),
+                "e2e": e2e, "gpu_launches": args.steps, "roofline": roofline,
+                "cpu_baseline": cpu, "clocks": clk}
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    run.release()
+    di.release()
+    dg.release()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return our_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

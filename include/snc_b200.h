@@ -112,6 +112,9 @@ typedef struct snc_b200_run snc_b200_run;       /* device-resident results of on
  * snc::cuda::available, src/runtime/cuda_backend.cu:181-184). */
 int snc_b200_available(void);
 int snc_b200_abi_version(void);
+/* Make `device` current for this host thread (the library links its own
+ * CUDA runtime, so a framework's current-device setting does not reach it). */
+int snc_b200_set_device(int device);
 /* Text of the last error on this host thread ("" if none). */
 const char* snc_b200_last_error(void);
 
@@ -135,6 +138,8 @@ int snc_b200_inputs_upload(const snc_b200_graph* g, const snc_input_event* event
                            size_t n_events, int32_t num_samples, const int32_t* steps,
                            snc_b200_inputs** out);
 int snc_b200_inputs_release(snc_b200_inputs* in);
+/* Bytes the schedule occupies on the device (= bytes copied host to device). */
+int snc_b200_inputs_info(const snc_b200_inputs* in, int64_t* device_bytes, int64_t* entries);
 
 /* ---- run --------------------------------------------------------------------
  * Run a batch on the device without host synchronisation.  stream is a
@@ -159,6 +164,9 @@ int snc_b200_run_fetch(snc_b200_run* r, float* logits, int64_t* spikes, int64_t*
                        uint32_t* raster, float* v_final, snc_run_stats* stats);
 /* The mode and path the last launch actually used (after AUTO resolution). */
 int snc_b200_run_used(const snc_b200_run* r, int* mode, int* path);
+/* 1 when the last launch went through the captured CUDA graph, 0 when it was
+ * launched directly (no SNC_B200_RUN_GRAPH, plain path, or capture refused). */
+int snc_b200_run_used_graph(const snc_b200_run* r);
 
 /* ---- one-call forward (the reference's cuda::forward, runtime.hpp:66-68) ---
  * One sample: events are that sample's InputEvents (sample_id ignored);

@@ -50,6 +50,8 @@ I32 = C.c_int32
 SIGNATURES = {
     "snc_b200_available": (C.c_int, []),
     "snc_b200_abi_version": (C.c_int, []),
+    "snc_b200_set_device": (C.c_int, [C.c_int]),
+    "snc_b200_inputs_info": (C.c_int, [P, P, P]),
     "snc_b200_last_error": (C.c_char_p, []),
     "snc_b200_graph_upload": (C.c_int, [P, P]),
     "snc_b200_graph_release": (C.c_int, [P]),
@@ -61,6 +63,7 @@ SIGNATURES = {
     "snc_b200_run_launch": (C.c_int, [P, P, C.c_int, C.c_int, P]),
     "snc_b200_run_fetch": (C.c_int, [P, P, P, P, P, P, P]),
     "snc_b200_run_used": (C.c_int, [P, P, P]),
+    "snc_b200_run_used_graph": (C.c_int, [P]),
     "snc_b200_forward": (C.c_int, [P, P, P, C.c_size_t, I32, P, C.c_int, P, P]),
     "snc_b200_forward_batched": (C.c_int, [P, P, C.c_size_t, I32, P, P, C.c_int, P, P, P, P]),
     "snc_b200_autotune": (C.c_int, [P, P, P, P, P, P]),

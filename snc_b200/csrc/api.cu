@@ -75,7 +75,7 @@ static void free_graph(Graph* g) {
   if (!g) return;
   for (void* p : {(void*)g->row_ptr, (void*)g->edges, (void*)g->post, (void*)g->col_of,
                   (void*)g->out_ch, (void*)g->role, (void*)g->channel, (void*)g->colbase,
-                  (void*)g->gedges, (void*)g->gptr, (void*)g->groups})
+                  (void*)g->gedges, (void*)g->gptr, (void*)g->groups, (void*)g->ibase})
     dev_free(p);
 }
 
@@ -180,6 +180,10 @@ static int upload_graph(const snc_graph_view* v, Graph* g) {
       gptr[i + 1] = (int)groups.size();
     }
   }
+  std::vector<int> ibase(P + 1, 0);
+  for (const int2& gr : groups) ibase[gr.x + 1]++;
+  for (int b = 0; b < P; ++b) ibase[b + 1] += ibase[b];
+  g->G = (int)groups.size();
   // fan-in skew and density for the autotuner signature
   {
     double mean = n ? (double)m / n : 0.0, var = 0.0;
@@ -204,6 +208,7 @@ static int upload_graph(const snc_graph_view* v, Graph* g) {
   if ((rc = dev_upload(&g->gedges, gedges.data(), gedges.size()))) return rc;
   if ((rc = dev_upload(&g->gptr, gptr.data(), gptr.size()))) return rc;
   if ((rc = dev_upload(&g->groups, groups.data(), groups.size()))) return rc;
+  if ((rc = dev_upload(&g->ibase, ibase.data(), ibase.size()))) return rc;
   return SNC_B200_OK;
 }
 
@@ -302,13 +307,35 @@ static int upload_inputs(const Graph* g, const snc_input_event* ev, size_t n_ev,
   if ((rc = dev_upload(&in->sched_nid, out_nid.data(), out_nid.size()))) return rc;
   if ((rc = dev_upload(&in->sched_ext, out_ext.data(), out_ext.size()))) return rc;
   if ((rc = dev_upload(&in->raster_off, in->raster_off_h.data(), (size_t)B))) return rc;
+  in->stepbase_h.assign(stepbase.begin(), stepbase.begin() + B);
+  if ((rc = dev_upload(&in->stepbase, in->stepbase_h.data(), (size_t)B))) return rc;
+  // first entry of every neuron block per step, for the multi-CTA kernels
+  const long long nblk = (long long)TS * (g->P + 1);
+  if (nblk > 0 && nblk <= (64ll << 20)) {
+    std::vector<int> blk((size_t)nblk);
+    for (int b = 0; b < B; ++b)
+      for (int t = 0; t < steps[b]; ++t) {
+        const long long gs = stepbase[b] + t;
+        const int k0 = sptr[in->sptr_off_h[b] + t], k1 = sptr[in->sptr_off_h[b] + t + 1];
+        int q = k0;
+        for (int p = 0; p <= g->P; ++p) {
+          const int lo = std::min(g->N, p * g->BS);
+          while (q < k1 && out_nid[q] < lo) ++q;
+          blk[(size_t)gs * (g->P + 1) + p] = (p == g->P) ? k1 : q;
+        }
+      }
+    if ((rc = dev_upload(&in->sched_blk, blk.data(), blk.size()))) return rc;
+    in->dev_bytes += (long long)blk.size() * 4;
+  }
+  in->dev_bytes += (long long)B * (4 + 4 + 8 + 8 + 8) + (long long)sptr.size() * 4 + in->n_entries * 8;
   return SNC_B200_OK;
 }
 
 static void free_inputs(Inputs* in) {
   if (!in) return;
   for (void* p : {(void*)in->steps, (void*)in->order, (void*)in->sptr_off, (void*)in->sched_ptr,
-                  (void*)in->sched_nid, (void*)in->sched_ext, (void*)in->raster_off})
+                  (void*)in->sched_nid, (void*)in->sched_ext, (void*)in->raster_off,
+                  (void*)in->stepbase, (void*)in->sched_blk})
     dev_free(p);
 }
 
@@ -317,10 +344,12 @@ static void free_run(Run* r) {
   if (r->gexec) cudaGraphExecDestroy(r->gexec);
   for (void* p : {(void*)r->counts, (void*)r->spikes, (void*)r->events, (void*)r->raster,
                   (void*)r->vfinal, (void*)r->err, (void*)r->ctl, (void*)r->v, (void*)r->refr,
-                  (void*)r->ring, (void*)r->fired, (void*)r->fired_cnt})
+                  (void*)r->ring, (void*)r->fired, (void*)r->fired_cnt, (void*)r->inbox,
+                  (void*)r->inbox_cnt})
     dev_free(p);
   if (r->ev0) cudaEventDestroy(r->ev0);
   if (r->ev1) cudaEventDestroy(r->ev1);
+  if (r->own_stream) cudaStreamDestroy(r->own_stream);
 }
 
 static int create_run(const Graph* g, const Inputs* in, int flags, Run* r) {
@@ -426,6 +455,11 @@ int snc_b200_available(void) { return check_device() == SNC_B200_OK ? 1 : 0; }
 
 int snc_b200_abi_version(void) { return SNC_B200_ABI_VERSION; }
 
+int snc_b200_set_device(int device) {
+  SNCB_CUDA(cudaSetDevice(device));
+  return SNC_B200_OK;
+}
+
 const char* snc_b200_last_error(void) { return g_last_error.c_str(); }
 
 int snc_b200_graph_upload(const snc_graph_view* v, snc_b200_graph** out) {
@@ -476,6 +510,13 @@ int snc_b200_inputs_release(snc_b200_inputs* in) {
   return SNC_B200_OK;
 }
 
+int snc_b200_inputs_info(const snc_b200_inputs* in, int64_t* device_bytes, int64_t* entries) {
+  if (!in) { set_error("null inputs"); return SNC_B200_EINVAL; }
+  if (device_bytes) *device_bytes = in->dev_bytes;
+  if (entries) *entries = in->n_entries;
+  return SNC_B200_OK;
+}
+
 int snc_b200_run_create(const snc_b200_graph* g, const snc_b200_inputs* in, int flags,
                         snc_b200_run** out) {
   if (!g || !in || !out || in->g != g) { set_error("bad run arguments"); return SNC_B200_EINVAL; }
@@ -510,6 +551,11 @@ int snc_b200_run_used(const snc_b200_run* r, int* mode, int* path) {
   if (mode) *mode = r->used_mode;
   if (path) *path = r->used_path;
   return SNC_B200_OK;
+}
+
+int snc_b200_run_used_graph(const snc_b200_run* r) {
+  if (!r) { set_error("null run"); return SNC_B200_EINVAL; }
+  return r->used_graph ? 1 : 0;
 }
 
 int snc_b200_forward(const snc_b200_graph* graph, const snc_graph_view* view,

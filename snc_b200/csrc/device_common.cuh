@@ -35,6 +35,16 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
   return v;
 }
 
+__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void fence_acq_rel_gpu() {
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
+}
+
 __device__ __forceinline__ int ld_volatile_i32(const int* p) {
   return *reinterpret_cast<const volatile int*>(p);
 }
@@ -104,22 +114,26 @@ __device__ __forceinline__ bool grid_sync(unsigned* ctr, unsigned target, int* e
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    __threadfence();
+    // release: the CTA's writes (ordered before this thread by bar.sync)
+    // become visible before the arrival is counted
     red_release_add_u32(ctr, 1u);
     int ok = 1;
-    const unsigned long long t0 = global_ns();
+    unsigned long long t0 = 0;
     unsigned spins = 0;
-    while (ld_acquire_u32(ctr) < target) {
-      if (ld_volatile_i32(err) != 0) { ok = 0; break; }
-      if ((++spins & 63u) == 0 && global_ns() - t0 > kSpinTimeoutNs) {
-        atomicCAS(err, 0, kErrTimeout);
-        ok = 0;
-        break;
+    while (ld_relaxed_u32(ctr) < target) {
+      if ((++spins & 255u) == 0) {
+        if (ld_volatile_i32(err) != 0) { ok = 0; break; }
+        const unsigned long long now = global_ns();
+        if (t0 == 0) t0 = now;
+        else if (now - t0 > kSpinTimeoutNs) {
+          atomicCAS(err, 0, kErrTimeout);
+          ok = 0;
+          break;
+        }
       }
-      __nanosleep(20);
     }
-    __threadfence();
-    s_ok = ok && ld_volatile_i32(err) == 0;
+    fence_acq_rel_gpu();  // acquire: later reads see the other CTAs' writes
+    s_ok = ok;
   }
   __syncthreads();
   return s_ok != 0;

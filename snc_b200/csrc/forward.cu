@@ -16,14 +16,23 @@
 //           and delay ring in shared memory; CTAs pull samples from a work
 //           queue (longest first), so uneven step counts balance across SMs.
 //   tier G  (k_tier_g)  every SM cooperates on a wave of samples in lockstep;
-//           CTA b owns neuron block b (its v, refr, ring columns) and a
-//           bounded software grid barrier separates the phases.
-//   plain   (k_plain_a / k_plain_b) the tier-G phases as one kernel launch
-//           each per step, one sample after another: the per-sample path.
+//           CTA b owns neuron block b: its v / refr and (SORT, BUCKET) its
+//           ring columns live in shared memory for the whole launch, and a
+//           bounded software grid barrier separates the two phases of a step.
+//   plain   (k_plain_a / k_plain_b) the same phases as one kernel launch
+//           each per step with state in global memory, one sample after
+//           another: the per-sample path.
 //
-// Delivery modes (include/snc_b200.h): ATOMIC red.add, BUCKET post-block
-// owner accumulates with atomics, SORT post-block owner applies each ring
-// cell's contributions in (pre, edge) order -- bit-identical to the CPU.
+// Delivery modes (include/snc_b200.h):
+//   ATOMIC  the owner of a fired neuron adds its row into the global ring
+//           with red.add (one barrier per step).
+//   BUCKET  the owner of a fired neuron posts one (first edge, length)
+//           descriptor per destination block to that block's inbox; after the
+//           barrier each block expands its inbox and accumulates into its
+//           shared-memory ring slice with shared atomics.
+//   SORT    as BUCKET, but the inbox is sorted by first edge and every ring
+//           cell receives its contributions in (pre, edge) order: the result
+//           is bit-identical to the serial CPU backend.
 #include <algorithm>
 #include <climits>
 #include <cstring>
@@ -36,9 +45,14 @@ namespace sncb {
 
 enum { MODE_ATOMIC = 0, MODE_BUCKET = 1, MODE_SORT = 2 };
 
+constexpr int kGThreads = 512;      // tier G / plain block size
+constexpr int kGChunk = 1024;       // staged events per ordered-apply chunk
+constexpr int kGDesc = 1024;        // inbox descriptors handled per chunk
+constexpr int kMaxWave = 64;        // samples per lockstep wave
+
 struct FwdArgs {
   // graph
-  int N, S, R, ncols, noc, P, BS;
+  int N, S, R, ncols, noc, P, BS, G;
   const int* row_ptr;
   const uint2* edges;
   const uint2* gedges;
@@ -47,14 +61,17 @@ struct FwdArgs {
   const int* col_of;
   const int* out_ch;
   const int* colbase;
+  const int* ibase;
   // inputs
   int B;
   const int* order;
   const int* steps;
   const long long* sptr_off;
+  const long long* stepbase;
   const int* sched_ptr;
   const int* sched_nid;
   const float* sched_ext;
+  const int* sched_blk;  // [total_steps][P+1] or null
   const long long* raster_off;
   // outputs
   int* counts;
@@ -63,24 +80,25 @@ struct FwdArgs {
   uint32_t* raster;
   float* vfinal;
   int W;
-  // grid state
+  // grid / plain state
   int Bw;
   float* v;
   int* refr;
   float* ring;
   int* fired;
   int* fired_cnt;
+  unsigned long long* inbox;  // [Bw][2][G]
+  int* inbox_cnt;             // [Bw][2][P]
   // control
   int* err;
   unsigned* ctl;
   LifP lif;
 };
 
-// Shared-memory bytes of the tier-S kernel for this graph (0 when the SORT
-// staging chunk is not needed).
+// Shared-memory bytes of the tier-S kernel for this graph.
 static size_t tier_s_bytes(int N, int ncols, int R, int noc, int mode, bool eprop, int nthr) {
   size_t words = (size_t)R * ncols + 4 * (size_t)N + (size_t)noc;
-  if (mode == MODE_SORT) words += (size_t)N + 1 + ncols + 3 * (size_t)nthr;
+  if (mode == MODE_SORT) words += (size_t)N + 1 + 2 * (size_t)ncols + 4 * (size_t)nthr;
   if (eprop) words += (size_t)N + ncols;
   return words * 4 + 16;
 }
@@ -114,33 +132,116 @@ __device__ __forceinline__ int ring_slot(int s0, int d, int R) {
   return s >= R ? s - R : s;
 }
 
-// Ordered apply of one chunk of staged events.  For every ring column with a
-// non-empty list, the contributions are added to their cells in increasing
-// staging index, i.e. in (pre, edge) order.  Lists are built with atomicExch
-// (arbitrary order) and replayed by repeated minimum selection.
 template <bool GLOBAL_RING>
-__device__ __forceinline__ void apply_ordered(int* head, int ncols_local, const int* st_slot,
-                                              const float* st_w, const int* st_next,
-                                              float* ring, int ring_stride, int col0) {
-  for (int c = threadIdx.x; c < ncols_local; c += blockDim.x) {
-    const int h = head[c];
-    if (h < 0) continue;
-    head[c] = -1;
-    int last = -1;
-    for (;;) {
-      int best = INT_MAX;
-      for (int p = h; p >= 0; p = st_next[p])
-        if (p > last && p < best) best = p;
-      if (best == INT_MAX) break;
-      float* cell = ring + (size_t)st_slot[best] * ring_stride + col0 + c;
-      if (GLOBAL_RING) {
-        __stcg(cell, __fadd_rn(__ldcg(cell), st_w[best]));
-      } else {
-        *cell = __fadd_rn(*cell, st_w[best]);
+__device__ __forceinline__ void apply_one(float* ring, int ring_stride, int col0, int c, int slot,
+                                          float w) {
+  float* cell = ring + (size_t)slot * ring_stride + col0 + c;
+  if (GLOBAL_RING) {
+    __stcg(cell, __fadd_rn(__ldcg(cell), w));
+  } else {
+    *cell = __fadd_rn(*cell, w);
+  }
+}
+
+// Tier S links chunks up to this many events in order with one warp; larger
+// chunks use unordered lists that every column sorts on its own.  Tier G
+// always links in order: its post blocks own hub columns whose per-step
+// event count can be large.
+constexpr int kSerialLinkMax = 192;
+constexpr int kRegSort = 8;
+
+// Ordered apply of one chunk of staged events.  Staging index q is the
+// (pre, edge) order of the CPU backend.  The events were staged with their
+// block-local column st_col[q] (head / tail of every local column = -1).
+// Every ring cell must receive its contributions in increasing q.
+//  - small chunks: one warp links the events of every column into a list in
+//    staging order, 32 events per step (match.any resolves same-column lanes);
+//    one thread per column then replays its list: O(events), no sorting, and
+//    hub columns with many events in one step stay linear.
+//  - large chunks: lists are built in parallel with atomicExch (arbitrary
+//    order); each column thread loads up to kRegSort list entries into
+//    registers, sorts them there and replays them; longer lists fall back to
+//    repeated minimum selection.
+template <bool GLOBAL_RING>
+__device__ void apply_ordered(int ce, int* head, int* tail, int ncols_local, const int* st_col,
+                              const int* st_slot, const float* st_w, int* st_next, float* ring,
+                              int ring_stride, int col0, int serial_max) {
+  __syncthreads();
+  if (ce > serial_max) {
+    for (int q = threadIdx.x; q < ce; q += blockDim.x) st_next[q] = atomicExch(&head[st_col[q]], q);
+    __syncthreads();
+    for (int c = threadIdx.x; c < ncols_local; c += blockDim.x) {
+      const int h = head[c];
+      if (h < 0) continue;
+      head[c] = -1;
+      int r[kRegSort];
+#pragma unroll
+      for (int i = 0; i < kRegSort; ++i) r[i] = INT_MAX;
+      int p = h;
+#pragma unroll
+      for (int i = 0; i < kRegSort; ++i) {
+        if (p >= 0) {
+          // insert p into the sorted r[0..kRegSort) (largest slot is free)
+          r[kRegSort - 1] = p;
+#pragma unroll
+          for (int k = kRegSort - 1; k > 0; --k) {
+            const int lo = min(r[k - 1], r[k]), hi = max(r[k - 1], r[k]);
+            r[k - 1] = lo;
+            r[k] = hi;
+          }
+          p = st_next[p];
+        }
       }
-      last = best;
+      if (p < 0) {
+#pragma unroll
+        for (int i = 0; i < kRegSort; ++i)
+          if (r[i] != INT_MAX) apply_one<GLOBAL_RING>(ring, ring_stride, col0, c, st_slot[r[i]], st_w[r[i]]);
+      } else {
+        int last = -1;
+        for (;;) {
+          int best = INT_MAX;
+          for (int x = h; x >= 0; x = st_next[x])
+            if (x > last && x < best) best = x;
+          if (best == INT_MAX) break;
+          apply_one<GLOBAL_RING>(ring, ring_stride, col0, c, st_slot[best], st_w[best]);
+          last = best;
+        }
+      }
+    }
+    __syncthreads();
+    return;
+  }
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    const unsigned below = (1u << lane) - 1u;
+    for (int g0 = 0; g0 < ce; g0 += 32) {
+      const int q = g0 + lane;
+      const bool valid = q < ce;
+      const int c = valid ? st_col[q] : -1 - lane;
+      const unsigned peers = __match_any_sync(0xffffffffu, c);
+      const unsigned lower = peers & below;
+      const bool last = (peers & ~below & ~(1u << lane)) == 0;
+      int t = -1;
+      if (valid && !lower) t = tail[c];
+      __syncwarp();
+      if (valid) {
+        if (lower) st_next[g0 + 31 - __clz(lower)] = q;
+        else if (t >= 0) st_next[t] = q;
+        else head[c] = q;
+        if (last) tail[c] = q;
+      }
+      __syncwarp();
     }
   }
+  __syncthreads();
+  for (int c = threadIdx.x; c < ncols_local; c += blockDim.x) {
+    int p = head[c];
+    if (p < 0) continue;
+    head[c] = -1;
+    tail[c] = -1;
+    for (; p >= 0; p = st_next[p]) apply_one<GLOBAL_RING>(ring, ring_stride, col0, c, st_slot[p], st_w[p]);
+  }
+  __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
@@ -164,7 +265,9 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
   int* counts = fired + N;
   int* pref = counts + noc;
   int* head = pref + (N + 1);
-  int* st_slot = head + nc;
+  int* tail = head + nc;
+  int* st_col = tail + nc;
+  int* st_slot = st_col + CH;
   float* st_w = reinterpret_cast<float*>(st_slot + CH);
   int* st_next = reinterpret_cast<int*>(st_w + CH);
 
@@ -183,7 +286,10 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
     }
     for (int i = tid; i < noc; i += nthr) counts[i] = 0;
     if (MODE == MODE_SORT)
-      for (int i = tid; i < nc; i += nthr) head[i] = -1;
+      for (int i = tid; i < nc; i += nthr) {
+        head[i] = -1;
+        tail[i] = -1;
+      }
     __syncthreads();
     const int* sp = a.sched_ptr + a.sptr_off[b];
     uint32_t* rast = a.raster ? a.raster + a.raster_off[b] : nullptr;
@@ -265,10 +371,12 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
             const uint2 ed = a.edges[a.row_ptr[fired[k]] + (e - pref[k])];
             st_slot[qq] = ring_slot(s0, edge_delay(ed), R);
             st_w[qq] = edge_w(ed);
-            st_next[qq] = atomicExch(&head[edge_col(ed)], qq);
+            st_col[qq] = edge_col(ed);
+            st_next[qq] = -1;
           }
           __syncthreads();
-          apply_ordered<false>(head, nc, st_slot, st_w, st_next, ring, nc, 0);
+          apply_ordered<false>(ce, head, tail, nc, st_col, st_slot, st_w, st_next, ring, nc, 0,
+                               kSerialLinkMax);
           __syncthreads();
         }
       }
@@ -291,85 +399,135 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
 // ---------------------------------------------------------------------------
 // tier G / plain: phases of one step for neuron block b of wave slot k
 // ---------------------------------------------------------------------------
+// Shared memory of a tier-G / plain CTA.  PERSIST (tier G) keeps v / refr
+// of its wave slots and cached row / group pointers of its neurons; RSM keeps
+// the ring columns of its block ([Bw][R][BS]) for SORT / BUCKET.
 struct GSmem {
-  float* ext;    // [BS]
-  int* fired;    // [BS]
-  int* pa;       // [P+1]
-  int* seg_s;    // [nthr]
-  int* seg_l;    // [nthr]
-  int* seg_p;    // [nthr]
-  int* head;     // [BS]
-  int* st_slot;  // [CH]
-  float* st_w;   // [CH]
-  int* st_next;  // [CH]
+  float* v;                  // PERSIST [Bw][BS]
+  int* refr;                 // PERSIST [Bw][BS]
+  int* col;                  // PERSIST [BS]   ring column (global index) or -1
+  int* rp;                   // PERSIST [BS+1] row_ptr of the block's neurons
+  int* gp;                   // PERSIST [BS+1] gptr of the block's neurons
+  float* ring;               // RSM [Bw][R][BS]
+  float* ext;                // [BS]
+  int* fired;                // [BS]
+  int* pa;                   // [P+1]
+  int* ib;                   // [P+1] inbox base of every destination block
+  int* head;                 // [BS]
+  int* tail;                 // [BS]
+  unsigned long long* desc;  // [kGDesc]
+  unsigned long long* dsort; // [kGDesc]
+  int* seg_p;                // [kGDesc]
+  int* st_col;               // [kGChunk]
+  int* st_slot;              // [kGChunk]
+  float* st_w;               // [kGChunk]
+  int* st_next;              // [kGChunk]
 };
 
-__device__ __forceinline__ GSmem carve_g(unsigned char* raw, int BS, int P, int nthr, int CH) {
-  GSmem s;
-  s.ext = reinterpret_cast<float*>(raw);
+static size_t g_smem_bytes(int BS, int P, int R, int Bw, bool persist, bool rsm) {
+  size_t b = 0;
+  b += 8 * (size_t)kGDesc * 2;                         // desc, dsort
+  b += 4 * ((size_t)BS * 4 + 2 * (P + 1) + kGDesc + 4 * (size_t)kGChunk);
+  if (persist) b += 4 * ((size_t)Bw * BS * 2 + BS + 2 * ((size_t)BS + 1));
+  if (rsm) b += 4 * (size_t)Bw * R * BS;
+  return b + 64;
+}
+
+__device__ __forceinline__ GSmem carve_g(unsigned char* raw, int BS, int P, int R, int Bw,
+                                         bool persist, bool rsm) {
+  GSmem s{};
+  s.desc = reinterpret_cast<unsigned long long*>(raw);
+  s.dsort = s.desc + kGDesc;
+  float* f = reinterpret_cast<float*>(s.dsort + kGDesc);
+  s.ext = f;
   s.fired = reinterpret_cast<int*>(s.ext + BS);
-  s.pa = s.fired + BS;
-  s.seg_s = s.pa + (P + 1);
-  s.seg_l = s.seg_s + nthr;
-  s.seg_p = s.seg_l + nthr;
-  s.head = s.seg_p + nthr;
-  s.st_slot = s.head + BS;
-  s.st_w = reinterpret_cast<float*>(s.st_slot + CH);
-  s.st_next = reinterpret_cast<int*>(s.st_w + CH);
+  s.head = s.fired + BS;
+  s.tail = s.head + BS;
+  s.pa = s.tail + BS;
+  s.ib = s.pa + (P + 1);
+  s.seg_p = s.ib + (P + 1);
+  s.st_col = s.seg_p + kGDesc;
+  s.st_slot = s.st_col + kGChunk;
+  s.st_w = reinterpret_cast<float*>(s.st_slot + kGChunk);
+  s.st_next = reinterpret_cast<int*>(s.st_w + kGChunk);
+  int* p = s.st_next + kGChunk;
+  if (persist) {
+    s.v = reinterpret_cast<float*>(p);
+    s.refr = reinterpret_cast<int*>(s.v + (size_t)Bw * BS);
+    s.col = s.refr + (size_t)Bw * BS;
+    s.rp = s.col + BS;
+    s.gp = s.rp + (BS + 1);
+    p = s.gp + (BS + 1);
+  }
+  if (rsm) s.ring = reinterpret_cast<float*>(p);
   return s;
 }
 
-static size_t tier_g_bytes(int BS, int P, int nthr) {
-  const int CH = nthr * 2;
-  return 4 * ((size_t)BS * 3 + (P + 1) + 3 * (size_t)nthr + 3 * (size_t)CH) + 16;
-}
-
-// Phase A: drive, integrate / fire own neurons, publish the ascending fired
-// list; in ATOMIC mode also deliver own fired rows into the (global) ring.
-template <int MODE>
+// Phase A: drive, integrate / fire the block's neurons, publish the ascending
+// fired list, then deliver (ATOMIC) or post inbox descriptors (BUCKET, SORT).
+template <int MODE, bool PERSIST, bool RSM>
 __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, long long* lsc, int k,
-                        int sample, int t, int b) {
+                        int sample, long long gstep, int t, int b, int cb0) {
   __shared__ int s_rng[2];
   const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = nthr >> 5;
   const int lo = b * a.BS, hi = min(a.N, lo + a.BS);
-  const int R = a.R, nc = a.ncols, N = a.N;
+  const int R = a.R, nc = a.ncols, N = a.N, BS = a.BS, P = a.P;
   const int par = t & 1;
   const int s0 = t % R;
-  float* ringk = a.ring + (size_t)k * R * nc;
-  float* vk = a.v + (size_t)k * N;
-  int* rk = a.refr + (size_t)k * N;
-  const int* sp = a.sched_ptr + a.sptr_off[sample];
-  for (int i = tid; i < hi - lo; i += nthr) sm.ext[i] = 0.f;
-  if (tid == 0) {
-    const int k0 = sp[t], k1 = sp[t + 1];
-    s_rng[0] = lower_bound_i(a.sched_nid, k0, k1, lo);
-    s_rng[1] = lower_bound_i(a.sched_nid, k0, k1, hi);
+  // this block's share of the step's injection schedule
+  int k0, k1;
+  if (a.sched_blk) {
+    const int* sb = a.sched_blk + gstep * (P + 1) + b;
+    k0 = sb[0];
+    k1 = sb[1];
+  } else {
+    if (tid == 0) {
+      const int* sp = a.sched_ptr + a.sptr_off[sample];
+      const int q0 = sp[t], q1 = sp[t + 1];
+      s_rng[0] = lower_bound_i(a.sched_nid, q0, q1, lo);
+      s_rng[1] = lower_bound_i(a.sched_nid, q0, q1, hi);
+    }
+    __syncthreads();
+    k0 = s_rng[0];
+    k1 = s_rng[1];
   }
-  __syncthreads();
-  for (int q = s_rng[0] + tid; q < s_rng[1]; q += nthr) sm.ext[a.sched_nid[q] - lo] = a.sched_ext[q];
+  for (int q = k0 + tid; q < k1; q += nthr) sm.ext[a.sched_nid[q] - lo] = a.sched_ext[q];
   __syncthreads();
   uint32_t* rast = a.raster ? a.raster + a.raster_off[sample] + (size_t)t * a.W : nullptr;
   int nf = 0;
   long long my_events = 0;
   for (int base = lo; base < hi; base += nthr) {
-    const int j = base + tid;
+    const int j = base + tid, jj = j - lo;
     int f = 0;
     if (j < hi) {
-      float vv = vk[j];
-      int rr = rk[j];
-      const int c = a.col_of[j];
+      float vv = PERSIST ? sm.v[k * BS + jj] : a.v[(size_t)k * N + j];
+      int rr = PERSIST ? sm.refr[k * BS + jj] : a.refr[(size_t)k * N + j];
+      const int c = PERSIST ? sm.col[jj] : a.col_of[j];
       float rin = 0.f;
       if (c >= 0) {
-        float* cell = ringk + (size_t)s0 * nc + c;
-        rin = __ldcg(cell);
-        __stcg(cell, 0.f);
+        if (RSM) {
+          float* cell = sm.ring + ((size_t)k * R + s0) * BS + (c - cb0);
+          rin = *cell;
+          *cell = 0.f;
+        } else {
+          float* cell = a.ring + ((size_t)k * R + s0) * nc + c;
+          rin = __ldcg(cell);
+          __stcg(cell, 0.f);
+        }
       }
-      f = lif_step(a.lif, vv, rr, sm.ext[j - lo], rin);
-      vk[j] = vv;
-      rk[j] = rr;
+      const float e = sm.ext[jj];
+      sm.ext[jj] = 0.f;
+      f = lif_step(a.lif, vv, rr, e, rin);
+      if (PERSIST) {
+        sm.v[k * BS + jj] = vv;
+        sm.refr[k * BS + jj] = rr;
+      } else {
+        a.v[(size_t)k * N + j] = vv;
+        a.refr[(size_t)k * N + j] = rr;
+      }
       if (f) {
-        my_events += a.row_ptr[j + 1] - a.row_ptr[j];
+        my_events += PERSIST ? sm.rp[jj + 1] - sm.rp[jj] : a.row_ptr[j + 1] - a.row_ptr[j];
         const int oc = a.out_ch[j];
         if (oc >= 0) atomicAdd(&a.counts[(size_t)sample * a.noc + oc], 1);
       }
@@ -386,16 +544,18 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, long lo
   for (int i = tid; i < nf; i += nthr) __stcg(&fo[i], sm.fired[i]);
   const long long ev = block_sum_ll(my_events, lsc);
   if (tid == 0) {
-    __stcg(&a.fired_cnt[((size_t)k * 2 + par) * a.P + b], nf);
+    __stcg(&a.fired_cnt[((size_t)k * 2 + par) * P + b], nf);
     if (nf) {
       atomicAdd(&a.spikes[sample], (unsigned long long)nf);
       atomicAdd(&a.events[sample], (unsigned long long)ev);
     }
   }
   if (MODE == MODE_ATOMIC) {
+    float* ringk = a.ring + (size_t)k * R * nc;
     for (int q = warp; q < nf; q += nwarps) {
       const int j = sm.fired[q];
-      const int rs = a.row_ptr[j], re = a.row_ptr[j + 1];
+      const int rs = PERSIST ? sm.rp[j - lo] : a.row_ptr[j];
+      const int re = PERSIST ? sm.rp[j - lo + 1] : a.row_ptr[j + 1];
       for (int e = (rs & ~1) + 2 * lane; e < re; e += 64) {
         const uint4 pr = *reinterpret_cast<const uint4*>(a.gedges + e);
         if (e >= rs) {
@@ -408,24 +568,50 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, long lo
         }
       }
     }
+  } else {
+    // one descriptor (first edge, length) per destination block of each
+    // fired row; a warp posts the groups of one row in parallel
+    int* cnt = a.inbox_cnt + ((size_t)k * 2 + par) * P;
+    unsigned long long* box = a.inbox + ((size_t)k * 2 + par) * a.G;
+    for (int q = warp; q < nf; q += nwarps) {
+      const int j = sm.fired[q];
+      const int g0 = PERSIST ? sm.gp[j - lo] : a.gptr[j];
+      const int g1 = PERSIST ? sm.gp[j - lo + 1] : a.gptr[j + 1];
+      const int re = PERSIST ? sm.rp[j - lo + 1] : a.row_ptr[j + 1];
+      for (int g = g0 + lane; g < g1; g += 32) {
+        const int2 gr = a.groups[g];
+        const int ge = (g + 1 < g1) ? a.groups[g + 1].y : re;
+        const int pos = atomicAdd(&cnt[gr.x], 1);
+        __stcg(&box[sm.ib[gr.x] + pos],
+               ((unsigned long long)(unsigned)gr.y << 32) | (unsigned)(ge - gr.y));
+      }
+    }
   }
   __syncthreads();
 }
 
-// Phase B (BUCKET / SORT): as owner of the ring columns of block b, gather the
-// row segments of every fired neuron that target this block, in ascending pre
-// order, and apply them.
-template <int MODE>
-__device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, int t, int b) {
+// Ring view of one wave slot for the post-owner phase: shared-memory slice
+// (local columns, stride BS) or the global ring (global columns, stride ncols).
+template <bool RSM>
+__device__ __forceinline__ float* ring_base(const FwdArgs& a, const GSmem& sm, int k) {
+  return RSM ? sm.ring + (size_t)k * a.R * a.BS : a.ring + (size_t)k * a.R * a.ncols;
+}
+
+// SORT fallback when a block's inbox exceeds kGDesc descriptors: walk every
+// block's ascending fired list (ascending pre order overall) and stage the
+// segments that target this block in that order.
+template <bool RSM>
+__device__ void phase_b_scan(const FwdArgs& a, const GSmem& sm, int* scratch, int k, int t, int b,
+                             int cb0, int cb1) {
   const int tid = threadIdx.x, nthr = blockDim.x;
-  const int CH = nthr * 2;
-  const int R = a.R, nc = a.ncols, P = a.P;
+  const int R = a.R, P = a.P;
   const int par = t & 1;
   const int s0 = t % R;
-  const int cb0 = a.colbase[b], cb1 = a.colbase[b + 1];
-  float* ringk = a.ring + (size_t)k * R * nc;
   const int* cntk = a.fired_cnt + ((size_t)k * 2 + par) * P;
   const int* fk = a.fired + ((size_t)k * 2 + par) * a.N;
+  float* rb = ring_base<RSM>(a, sm, k);
+  const int stride = RSM ? a.BS : a.ncols;
+  const int col0 = RSM ? 0 : cb0;
   int F;
   {
     const int cnt = tid < P ? __ldcg(&cntk[tid]) : 0;
@@ -433,7 +619,8 @@ __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, 
     if (tid < P) sm.pa[tid] = ex;
     __syncthreads();
   }
-  if (cb1 == cb0 || F == 0) return;
+  int* seg_s = reinterpret_cast<int*>(sm.desc);
+  int* seg_l = reinterpret_cast<int*>(sm.dsort);
   for (int f0 = 0; f0 < F; f0 += nthr) {
     const int f = f0 + tid;
     int gs = 0, gl = 0;
@@ -456,126 +643,230 @@ __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, 
     unsigned m;
     const int pos = ballot_compact(gl > 0, scratch, &nseg, &m);
     if (gl > 0) {
-      sm.seg_s[pos] = gs;
-      sm.seg_l[pos] = gl;
+      seg_s[pos] = gs;
+      seg_l[pos] = gl;
     }
     __syncthreads();
     int E;
     {
-      const int len = tid < nseg ? sm.seg_l[tid] : 0;
+      const int len = tid < nseg ? seg_l[tid] : 0;
       const int ex = block_exclusive_scan(len, scratch, &E);
       if (tid < nseg) sm.seg_p[tid] = ex;
       __syncthreads();
     }
-    for (int e0 = 0; e0 < E; e0 += CH) {
-      const int ce = min(CH, E - e0);
+    for (int e0 = 0; e0 < E; e0 += kGChunk) {
+      const int ce = min(kGChunk, E - e0);
       for (int qq = tid; qq < ce; qq += nthr) {
         const int e = e0 + qq;
         const int s = upper_index(sm.seg_p, nseg, e);
-        const uint2 ed = a.gedges[sm.seg_s[s] + (e - sm.seg_p[s])];
+        const uint2 ed = a.gedges[seg_s[s] + (e - sm.seg_p[s])];
+        sm.st_slot[qq] = ring_slot(s0, edge_delay(ed), R);
+        sm.st_w[qq] = edge_w(ed);
+        sm.st_col[qq] = edge_col(ed) - cb0;
+        sm.st_next[qq] = -1;
+      }
+      apply_ordered<!RSM>(ce, sm.head, sm.tail, cb1 - cb0, sm.st_col, sm.st_slot, sm.st_w,
+                          sm.st_next, rb, stride, col0, kGChunk);
+    }
+  }
+}
+
+// Phase B (BUCKET / SORT): as owner of the ring columns of block b, expand
+// this step's inbox descriptors and accumulate them into the block's ring
+// slice -- unordered (BUCKET) or per ring cell in (pre, edge) order (SORT).
+template <int MODE, bool RSM>
+__device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, int t, int b,
+                        int cb0, int cb1) {
+  __shared__ int s_cnt;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int R = a.R;
+  const int par = t & 1;
+  const int s0 = t % R;
+  int* cntp = a.inbox_cnt + ((size_t)k * 2 + par) * a.P + b;
+  if (tid == 0) {
+    s_cnt = __ldcg(cntp);
+    // reset for step t + 2 (written again only after the next grid barrier)
+    if (s_cnt) __stcg(cntp, 0);
+  }
+  __syncthreads();
+  const int cnt = s_cnt;
+  if (cnt == 0) return;
+  if (MODE == MODE_SORT && cnt > kGDesc) {
+    phase_b_scan<RSM>(a, sm, scratch, k, t, b, cb0, cb1);
+    return;
+  }
+  float* rb = ring_base<RSM>(a, sm, k);
+  const int stride = RSM ? a.BS : a.ncols;
+  const int col0 = RSM ? 0 : cb0;
+  const unsigned long long* box = a.inbox + ((size_t)k * 2 + par) * a.G + a.ibase[b];
+  for (int d0 = 0; d0 < cnt; d0 += kGDesc) {
+    const int dn = min(kGDesc, cnt - d0);
+    for (int i = tid; i < dn; i += nthr) sm.desc[i] = __ldcg(&box[d0 + i]);
+    __syncthreads();
+    const unsigned long long* src = sm.desc;
+    if (MODE == MODE_SORT) {
+      // rank sort by first edge (first edges of distinct rows are distinct)
+      for (int i = tid; i < dn; i += nthr) {
+        const unsigned long long key = sm.desc[i];
+        int r = 0;
+        for (int q = 0; q < dn; ++q) r += (sm.desc[q] >> 32) < (key >> 32);
+        sm.dsort[r] = key;
+      }
+      __syncthreads();
+      src = sm.dsort;
+    }
+    // prefix of segment lengths, two descriptors per thread
+    int E;
+    {
+      const int i0 = 2 * tid, i1 = 2 * tid + 1;
+      const int l0 = i0 < dn ? (int)(src[i0] & 0xffffffffu) : 0;
+      const int l1 = i1 < dn ? (int)(src[i1] & 0xffffffffu) : 0;
+      const int ex = block_exclusive_scan(l0 + l1, scratch, &E);
+      if (i0 < dn) sm.seg_p[i0] = ex;
+      if (i1 < dn) sm.seg_p[i1] = ex + l0;
+      __syncthreads();
+    }
+    for (int e0 = 0; e0 < E; e0 += kGChunk) {
+      const int ce = min(kGChunk, E - e0);
+      for (int qq = tid; qq < ce; qq += nthr) {
+        const int e = e0 + qq;
+        const int d = upper_index(sm.seg_p, dn, e);
+        const int edge = (int)(src[d] >> 32) + (e - sm.seg_p[d]);
+        const uint2 ed = a.gedges[edge];
         const int slot = ring_slot(s0, edge_delay(ed), R);
         if (MODE == MODE_BUCKET) {
-          atomicAdd(&ringk[(size_t)slot * nc + edge_col(ed)], edge_w(ed));
+          // shared slice: block-local column; global ring: global column
+          const int cidx = RSM ? edge_col(ed) - cb0 : edge_col(ed);
+          atomicAdd(&rb[(size_t)slot * stride + cidx], edge_w(ed));
         } else {
           sm.st_slot[qq] = slot;
           sm.st_w[qq] = edge_w(ed);
-          sm.st_next[qq] = atomicExch(&sm.head[edge_col(ed) - cb0], qq);
+          sm.st_col[qq] = edge_col(ed) - cb0;
+          sm.st_next[qq] = -1;
         }
       }
-      __syncthreads();
       if (MODE == MODE_SORT) {
-        apply_ordered<true>(sm.head, cb1 - cb0, sm.st_slot, sm.st_w, sm.st_next, ringk, nc, cb0);
+        apply_ordered<!RSM>(ce, sm.head, sm.tail, cb1 - cb0, sm.st_col, sm.st_slot, sm.st_w,
+                            sm.st_next, rb, stride, col0, kGChunk);
+      } else {
         __syncthreads();
       }
     }
   }
 }
 
-// Zero the state a CTA owns for wave slot k: v / refr of its neurons and its
-// ring columns in every slot.
-__device__ void init_block_state(const FwdArgs& a, int k, int b) {
-  const int lo = b * a.BS, hi = min(a.N, lo + a.BS);
-  const int cb0 = a.colbase[b], cb1 = a.colbase[b + 1];
-  float* vk = a.v + (size_t)k * a.N;
-  int* rk = a.refr + (size_t)k * a.N;
-  for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
-    vk[j] = 0.f;
-    rk[j] = 0;
-  }
-  float* ringk = a.ring + (size_t)k * a.R * a.ncols;
-  const int w = cb1 - cb0;
-  for (int i = threadIdx.x; i < a.R * w; i += blockDim.x)
-    __stcg(&ringk[(size_t)(i / w) * a.ncols + cb0 + (i % w)], 0.f);
-}
-
-template <int MODE>
-__global__ void __launch_bounds__(512, 1) k_tier_g(FwdArgs a) {
+template <int MODE, bool RSM>
+__global__ void __launch_bounds__(kGThreads, 1) k_tier_g(FwdArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int scratch[40];
   __shared__ long long lscratch[40];
-  const GSmem sm = carve_g(smem_raw, a.BS, a.P, blockDim.x, blockDim.x * 2);
+  __shared__ int s_samp[kMaxWave], s_T[kMaxWave];
+  __shared__ long long s_gb[kMaxWave];
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const GSmem sm = carve_g(smem_raw, a.BS, a.P, a.R, a.Bw, true, RSM);
   const int b = blockIdx.x;
+  const int BS = a.BS, R = a.R;
+  const int lo = b * BS, hi = min(a.N, lo + BS);
+  const int cb0 = a.colbase[b], cb1 = a.colbase[b + 1];
   const unsigned nb = gridDim.x;
   unsigned target = 0;
+  for (int jj = tid; jj < BS; jj += nthr) {
+    sm.col[jj] = lo + jj < hi ? a.col_of[lo + jj] : -1;
+    sm.ext[jj] = 0.f;
+    sm.head[jj] = -1;
+    sm.tail[jj] = -1;
+  }
+  for (int jj = tid; jj <= BS; jj += nthr) {
+    const int j = min(lo + jj, hi);
+    sm.rp[jj] = a.row_ptr[j];
+    sm.gp[jj] = a.gptr[j];
+  }
+  for (int i = tid; i <= a.P; i += nthr) sm.ib[i] = a.ibase[i];
   const int nwaves = (a.B + a.Bw - 1) / a.Bw;
-  if (MODE == MODE_SORT)
-    for (int i = threadIdx.x; i < a.BS; i += blockDim.x) sm.head[i] = -1;
   for (int w = 0; w < nwaves; ++w) {
     const int q0 = w * a.Bw;
     const int nk = min(a.Bw, a.B - q0);
-    for (int k = 0; k < nk; ++k) init_block_state(a, k, b);
-    const int Tw = a.steps[a.order[q0]];
+    if (tid < nk) {
+      const int smp = a.order[q0 + tid];
+      s_samp[tid] = smp;
+      s_T[tid] = a.steps[smp];
+      s_gb[tid] = a.stepbase[smp];
+    }
+    for (int i = tid; i < nk * BS; i += nthr) {
+      sm.v[i] = 0.f;
+      sm.refr[i] = 0;
+    }
+    if (RSM) {
+      for (int i = tid; i < nk * R * BS; i += nthr) sm.ring[i] = 0.f;
+    } else {
+      const int wcol = cb1 - cb0;
+      for (int k = 0; k < nk; ++k) {
+        float* ringk = a.ring + (size_t)k * R * a.ncols;
+        for (int i = tid; i < R * wcol; i += nthr)
+          __stcg(&ringk[(size_t)(i / wcol) * a.ncols + cb0 + (i % wcol)], 0.f);
+      }
+    }
     target += nb;
     if (!grid_sync(&a.ctl[0], target, a.err)) return;
+    const int Tw = s_T[0];
     for (int t = 0; t < Tw; ++t) {
-      for (int k = 0; k < nk; ++k) {
-        const int smp = a.order[q0 + k];
-        if (t < a.steps[smp]) phase_a<MODE>(a, sm, scratch, lscratch, k, smp, t, b);
-      }
+      for (int k = 0; k < nk; ++k)
+        if (t < s_T[k])
+          phase_a<MODE, true, RSM>(a, sm, scratch, lscratch, k, s_samp[k], s_gb[k] + t, t, b, cb0);
       target += nb;
       if (!grid_sync(&a.ctl[0], target, a.err)) return;
-      if (MODE != MODE_ATOMIC) {
-        for (int k = 0; k < nk; ++k) {
-          const int smp = a.order[q0 + k];
-          if (t < a.steps[smp]) phase_b<MODE>(a, sm, scratch, k, t, b);
-        }
-      }
+      if (MODE != MODE_ATOMIC)
+        for (int k = 0; k < nk; ++k)
+          if (t < s_T[k]) phase_b<MODE, RSM>(a, sm, scratch, k, t, b, cb0, cb1);
     }
-    if (a.vfinal) {
-      const int lo = b * a.BS, hi = min(a.N, lo + a.BS);
-      for (int k = 0; k < nk; ++k) {
-        const int smp = a.order[q0 + k];
-        for (int j = lo + threadIdx.x; j < hi; j += blockDim.x)
-          a.vfinal[(size_t)smp * a.N + j] = a.v[(size_t)k * a.N + j];
-      }
-    }
+    if (a.vfinal)
+      for (int k = 0; k < nk; ++k)
+        for (int j = lo + tid; j < hi; j += nthr)
+          a.vfinal[(size_t)s_samp[k] * a.N + j] = sm.v[k * BS + (j - lo)];
     target += nb;
     if (!grid_sync(&a.ctl[0], target, a.err)) return;
   }
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(512) k_plain_a(FwdArgs a, int sample, int t) {
+__global__ void __launch_bounds__(kGThreads) k_plain_a(FwdArgs a, int sample, long long gstep, int t) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int scratch[40];
   __shared__ long long lscratch[40];
-  const GSmem sm = carve_g(smem_raw, a.BS, a.P, blockDim.x, blockDim.x * 2);
-  phase_a<MODE>(a, sm, scratch, lscratch, 0, sample, t, blockIdx.x);
+  const GSmem sm = carve_g(smem_raw, a.BS, a.P, a.R, 1, false, false);
+  for (int jj = threadIdx.x; jj < a.BS; jj += blockDim.x) sm.ext[jj] = 0.f;
+  for (int i = threadIdx.x; i <= a.P; i += blockDim.x) sm.ib[i] = a.ibase[i];
+  __syncthreads();
+  phase_a<MODE, false, false>(a, sm, scratch, lscratch, 0, sample, gstep, t, blockIdx.x,
+                              a.colbase[blockIdx.x]);
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(512) k_plain_b(FwdArgs a, int t) {
+__global__ void __launch_bounds__(kGThreads) k_plain_b(FwdArgs a, int t) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int scratch[40];
-  const GSmem sm = carve_g(smem_raw, a.BS, a.P, blockDim.x, blockDim.x * 2);
-  if (MODE == MODE_SORT)
-    for (int i = threadIdx.x; i < a.BS; i += blockDim.x) sm.head[i] = -1;
+  const GSmem sm = carve_g(smem_raw, a.BS, a.P, a.R, 1, false, false);
+  for (int jj = threadIdx.x; jj < a.BS; jj += blockDim.x) {
+    sm.head[jj] = -1;
+    sm.tail[jj] = -1;
+  }
   __syncthreads();
-  phase_b<MODE>(a, sm, scratch, 0, t, blockIdx.x);
+  phase_b<MODE, false>(a, sm, scratch, 0, t, blockIdx.x, a.colbase[blockIdx.x],
+                       a.colbase[blockIdx.x + 1]);
 }
 
+// Zero wave slot 0's global state of block b (plain path, once per sample).
 __global__ void k_plain_init(FwdArgs a) {
-  init_block_state(a, 0, blockIdx.x);
+  const int b = blockIdx.x;
+  const int lo = b * a.BS, hi = min(a.N, lo + a.BS);
+  const int cb0 = a.colbase[b], cb1 = a.colbase[b + 1];
+  for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+    a.v[j] = 0.f;
+    a.refr[j] = 0;
+  }
+  const int w = cb1 - cb0;
+  for (int i = threadIdx.x; i < a.R * w; i += blockDim.x)
+    a.ring[(size_t)(i / w) * a.ncols + cb0 + (i % w)] = 0.f;
 }
 
 __global__ void k_copy_v(FwdArgs a, int sample) {
@@ -591,36 +882,55 @@ static FwdArgs make_args(Run* r, const snc_lif* lif) {
   const Inputs* in = r->in;
   FwdArgs a{};
   a.N = g->N; a.S = g->S; a.R = g->R; a.ncols = g->ncols; a.noc = std::max(1, g->noc);
-  a.P = g->P; a.BS = g->BS;
+  a.P = g->P; a.BS = g->BS; a.G = g->G;
   a.row_ptr = g->row_ptr; a.edges = g->edges; a.gedges = g->gedges; a.gptr = g->gptr;
   a.groups = g->groups; a.col_of = g->col_of; a.out_ch = g->out_ch; a.colbase = g->colbase;
+  a.ibase = g->ibase;
   a.B = in->B; a.order = in->order; a.steps = in->steps; a.sptr_off = in->sptr_off;
+  a.stepbase = in->stepbase;
   a.sched_ptr = in->sched_ptr; a.sched_nid = in->sched_nid; a.sched_ext = in->sched_ext;
+  a.sched_blk = in->sched_blk;
   a.raster_off = in->raster_off;
   a.counts = r->counts; a.spikes = r->spikes; a.events = r->events;
   a.raster = (r->flags & SNC_B200_RUN_RASTER) ? r->raster : nullptr;
   a.vfinal = (r->flags & SNC_B200_RUN_VFINAL) ? r->vfinal : nullptr;
   a.W = r->W;
   a.Bw = r->Bw; a.v = r->v; a.refr = r->refr; a.ring = r->ring; a.fired = r->fired;
-  a.fired_cnt = r->fired_cnt;
+  a.fired_cnt = r->fired_cnt; a.inbox = r->inbox; a.inbox_cnt = r->inbox_cnt;
   a.err = r->err; a.ctl = r->ctl;
   a.lif = LifP{lif->threshold, lif->decay, lif->reset, lif->refractory, lif->reset_mode};
   return a;
 }
 
 static int ensure_grid_state(Run* r, int Bw) {
-  if (r->v && r->Bw >= Bw) return SNC_B200_OK;
+  if (r->v && r->Bw_cap >= Bw) {
+    r->Bw = Bw;
+    return SNC_B200_OK;
+  }
   const Graph* g = r->g;
-  dev_free(r->v); dev_free(r->refr); dev_free(r->ring); dev_free(r->fired); dev_free(r->fired_cnt);
-  r->v = nullptr; r->refr = nullptr; r->ring = nullptr; r->fired = nullptr; r->fired_cnt = nullptr;
+  for (void* p : {(void*)r->v, (void*)r->refr, (void*)r->ring, (void*)r->fired,
+                  (void*)r->fired_cnt, (void*)r->inbox, (void*)r->inbox_cnt})
+    dev_free(p);
+  r->v = nullptr; r->refr = nullptr; r->ring = nullptr; r->fired = nullptr;
+  r->fired_cnt = nullptr; r->inbox = nullptr; r->inbox_cnt = nullptr;
   int rc;
   if ((rc = dev_alloc(&r->v, (size_t)Bw * g->N))) return rc;
   if ((rc = dev_alloc(&r->refr, (size_t)Bw * g->N))) return rc;
   if ((rc = dev_alloc(&r->ring, (size_t)Bw * g->R * std::max(1, g->ncols)))) return rc;
   if ((rc = dev_alloc(&r->fired, (size_t)Bw * 2 * g->N))) return rc;
   if ((rc = dev_alloc(&r->fired_cnt, (size_t)Bw * 2 * g->P))) return rc;
+  if ((rc = dev_alloc(&r->inbox, (size_t)Bw * 2 * std::max(1, g->G)))) return rc;
+  if ((rc = dev_alloc(&r->inbox_cnt, (size_t)Bw * 2 * g->P))) return rc;
   r->Bw = Bw;
+  r->Bw_cap = Bw;
   return SNC_B200_OK;
+}
+
+static int optin_smem() {
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  return optin;
 }
 
 template <int MODE>
@@ -641,14 +951,41 @@ static int launch_tier_s(Run* r, const FwdArgs& a, cudaStream_t st) {
   return SNC_B200_OK;
 }
 
-template <int MODE>
-static int launch_tier_g(Run* r, const FwdArgs& a, cudaStream_t st) {
+// Wave size and ring placement of the tier-G kernel for this run.
+struct GPlan {
+  bool rsm;
+  int Bw;
+  size_t smem;
+};
+
+static GPlan plan_tier_g(const Graph* g, int B, int mode) {
+  const size_t optin = (size_t)optin_smem();
+  GPlan p{false, 1, 0};
+  const int cap = std::max(1, std::min(B, kMaxWave));
+  if (mode != MODE_ATOMIC) {
+    int bw = 0;
+    while (bw < cap && g_smem_bytes(g->BS, g->P, g->R, bw + 1, true, true) <= optin) ++bw;
+    if (bw >= 1) {
+      p.rsm = true;
+      p.Bw = bw;
+    }
+  }
+  if (!p.rsm) {
+    int bw = 0;
+    while (bw < cap && g_smem_bytes(g->BS, g->P, g->R, bw + 1, true, false) <= optin) ++bw;
+    p.Bw = std::max(1, bw);
+  }
+  p.smem = g_smem_bytes(g->BS, g->P, g->R, p.Bw, true, p.rsm);
+  return p;
+}
+
+template <int MODE, bool RSM>
+static int launch_tier_g(Run* r, const FwdArgs& a, size_t smem, cudaStream_t st) {
   const Graph* g = r->g;
-  const int nthr = 512;
-  const size_t smem = tier_g_bytes(g->BS, g->P, nthr);
-  SNCB_CUDA(cudaFuncSetAttribute(k_tier_g<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int nthr = kGThreads;
+  SNCB_CUDA(cudaFuncSetAttribute(k_tier_g<MODE, RSM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  SNCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tier_g<MODE>, nthr, smem));
+  SNCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tier_g<MODE, RSM>, nthr, smem));
   if (per_sm * g->sm_count < g->P) {
     set_error("grid tier: blocks cannot be co-resident");
     return SNC_B200_EUNSUPPORTED;
@@ -663,7 +1000,7 @@ static int launch_tier_g(Run* r, const FwdArgs& a, cudaStream_t st) {
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  SNCB_CUDA(cudaLaunchKernelEx(&cfg, k_tier_g<MODE>, a));
+  SNCB_CUDA(cudaLaunchKernelEx(&cfg, k_tier_g<MODE, RSM>, a));
   return SNC_B200_OK;
 }
 
@@ -671,16 +1008,17 @@ template <int MODE>
 static int launch_plain(Run* r, FwdArgs a, cudaStream_t st) {
   const Graph* g = r->g;
   const Inputs* in = r->in;
-  const int nthr = 512;
-  const size_t smem = tier_g_bytes(g->BS, g->P, nthr);
+  const int nthr = kGThreads;
+  const size_t smem = g_smem_bytes(g->BS, g->P, g->R, 1, false, false);
   SNCB_CUDA(cudaFuncSetAttribute(k_plain_a<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   SNCB_CUDA(cudaFuncSetAttribute(k_plain_b<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (int q = 0; q < in->B; ++q) {
     const int smp = in->order_h[q];
     const int T = in->steps_h[smp];
+    const long long gb = in->stepbase_h[smp];
     k_plain_init<<<g->P, nthr, 0, st>>>(a);
     for (int t = 0; t < T; ++t) {
-      k_plain_a<MODE><<<g->P, nthr, smem, st>>>(a, smp, t);
+      k_plain_a<MODE><<<g->P, nthr, smem, st>>>(a, smp, gb + t, t);
       if (MODE != MODE_ATOMIC) k_plain_b<MODE><<<g->P, nthr, smem, st>>>(a, t);
     }
     if (a.vfinal) k_copy_v<<<std::max(1, std::min(1024, (g->N + 255) / 256)), 256, 0, st>>>(a, smp);
@@ -690,24 +1028,30 @@ static int launch_plain(Run* r, FwdArgs a, cudaStream_t st) {
 }
 
 static bool tier_s_fits(const Graph* g, int mode) {
-  int dev = 0, optin = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  return tier_s_bytes(g->N, g->ncols, g->R, std::max(1, g->noc), mode, false, 1024) <= (size_t)optin;
+  return tier_s_bytes(g->N, g->ncols, g->R, std::max(1, g->noc), mode, false, 1024) <=
+         (size_t)optin_smem();
+}
+
+static bool use_tier_s(const Run* r, int mode, int path) {
+  return path == SNC_B200_PATH_PERSISTENT && tier_s_fits(r->g, mode) &&
+         !(r->flags & SNC_B200_RUN_FORCE_GRID);
 }
 
 // Launch body without timing / graph handling.
 static int launch_body(Run* r, const FwdArgs& a, int mode, int path, cudaStream_t st) {
-  const Graph* g = r->g;
-  if (path == SNC_B200_PATH_PERSISTENT && tier_s_fits(g, mode) &&
-      !(r->flags & SNC_B200_RUN_FORCE_GRID)) {
+  if (use_tier_s(r, mode, path)) {
     if (mode == MODE_SORT) return launch_tier_s<MODE_SORT>(r, a, st);
     return launch_tier_s<MODE_ATOMIC>(r, a, st);
   }
   if (path == SNC_B200_PATH_PERSISTENT) {
-    if (mode == MODE_SORT) return launch_tier_g<MODE_SORT>(r, a, st);
-    if (mode == MODE_BUCKET) return launch_tier_g<MODE_BUCKET>(r, a, st);
-    return launch_tier_g<MODE_ATOMIC>(r, a, st);
+    const size_t smem = r->gplan_smem;
+    if (mode == MODE_ATOMIC) return launch_tier_g<MODE_ATOMIC, false>(r, a, smem, st);
+    if (r->gplan_rsm) {
+      if (mode == MODE_SORT) return launch_tier_g<MODE_SORT, true>(r, a, smem, st);
+      return launch_tier_g<MODE_BUCKET, true>(r, a, smem, st);
+    }
+    if (mode == MODE_SORT) return launch_tier_g<MODE_SORT, false>(r, a, smem, st);
+    return launch_tier_g<MODE_BUCKET, false>(r, a, smem, st);
   }
   if (mode == MODE_SORT) return launch_plain<MODE_SORT>(r, a, st);
   if (mode == MODE_BUCKET) return launch_plain<MODE_BUCKET>(r, a, st);
@@ -728,30 +1072,39 @@ int launch_run(Run* r, const snc_lif* lif, int mode, int path, cudaStream_t st) 
     set_error("bad mode or path");
     return SNC_B200_EINVAL;
   }
-  const bool tier_s = path == SNC_B200_PATH_PERSISTENT && tier_s_fits(g, mode) &&
-                      !(r->flags & SNC_B200_RUN_FORCE_GRID);
   int rc;
-  if (!tier_s) {
+  if (!use_tier_s(r, mode, path)) {
     int Bw = 1;
     if (path == SNC_B200_PATH_PERSISTENT) {
-      // lockstep wave size: bounded by a 4 GiB state budget and 64 samples
-      const size_t per = (size_t)4 * ((size_t)g->R * std::max(1, g->ncols) + 4 * (size_t)g->N);
-      Bw = (int)std::max<size_t>(1, std::min<size_t>({(size_t)in->B, (size_t)64, ((size_t)4 << 30) / per}));
+      const GPlan p = plan_tier_g(g, in->B, mode);
+      Bw = p.Bw;
+      r->gplan_rsm = p.rsm;
+      r->gplan_smem = p.smem;
     }
     if ((rc = ensure_grid_state(r, Bw))) return rc;
   }
   const FwdArgs a = make_args(r, lif);
   const size_t B = (size_t)std::max(1, in->B);
+  // The legacy default stream cannot be captured; a run owns a blocking
+  // stream (ordered with the legacy stream) that stands in for it.
+  if (!st) {
+    if (!r->own_stream) SNCB_CUDA(cudaStreamCreate(&r->own_stream));
+    st = r->own_stream;
+  }
   SNCB_CUDA(cudaMemsetAsync(r->counts, 0, B * std::max(1, g->noc) * sizeof(int), st));
   SNCB_CUDA(cudaMemsetAsync(r->spikes, 0, B * sizeof(unsigned long long), st));
   SNCB_CUDA(cudaMemsetAsync(r->events, 0, B * sizeof(unsigned long long), st));
   SNCB_CUDA(cudaMemsetAsync(r->ctl, 0, 4 * sizeof(unsigned), st));
   SNCB_CUDA(cudaMemsetAsync(r->err, 0, sizeof(int), st));
+  if (r->inbox_cnt)
+    SNCB_CUDA(cudaMemsetAsync(r->inbox_cnt, 0, (size_t)r->Bw_cap * 2 * g->P * sizeof(int), st));
   if ((r->flags & SNC_B200_RUN_RASTER) && in->raster_words)
     SNCB_CUDA(cudaMemsetAsync(r->raster, 0, (size_t)in->raster_words * sizeof(uint32_t), st));
   SNCB_CUDA(cudaEventRecord(r->ev0, st));
+  r->used_graph = false;
   if (in->B > 0) {
-    const bool use_graph = (r->flags & SNC_B200_RUN_GRAPH) && path == SNC_B200_PATH_PERSISTENT;
+    bool use_graph = (r->flags & SNC_B200_RUN_GRAPH) && path == SNC_B200_PATH_PERSISTENT &&
+                     !r->graph_refused;
     if (use_graph) {
       const bool same = r->gexec && r->gexec_mode == mode && r->gexec_stream == st &&
                         std::memcmp(&r->gexec_lif, lif, sizeof(snc_lif)) == 0;
@@ -759,19 +1112,33 @@ int launch_run(Run* r, const snc_lif* lif, int mode, int path, cudaStream_t st) 
         if (r->gexec) cudaGraphExecDestroy(r->gexec);
         r->gexec = nullptr;
         cudaGraph_t cg = nullptr;
-        SNCB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        rc = launch_body(r, a, mode, path, st);
-        cudaError_t ce = cudaStreamEndCapture(st, &cg);
-        if (rc) { if (cg) cudaGraphDestroy(cg); return rc; }
-        if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
-        ce = cudaGraphInstantiate(&r->gexec, cg, 0);
-        cudaGraphDestroy(cg);
-        if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
-        r->gexec_mode = mode;
-        r->gexec_lif = *lif;
-        r->gexec_stream = st;
+        cudaError_t ce = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        if (ce == cudaSuccess) {
+          rc = launch_body(r, a, mode, path, st);
+          ce = cudaStreamEndCapture(st, &cg);
+          if (rc) {
+            if (cg) cudaGraphDestroy(cg);
+            return rc;
+          }
+          if (ce == cudaSuccess) ce = cudaGraphInstantiate(&r->gexec, cg, 0);
+          if (cg) cudaGraphDestroy(cg);
+        }
+        if (ce != cudaSuccess) {
+          // capture refused: remember it and launch directly from now on
+          cudaGetLastError();
+          r->gexec = nullptr;
+          r->graph_refused = true;
+          use_graph = false;
+        } else {
+          r->gexec_mode = mode;
+          r->gexec_lif = *lif;
+          r->gexec_stream = st;
+        }
       }
+    }
+    if (use_graph) {
       SNCB_CUDA(cudaGraphLaunch(r->gexec, st));
+      r->used_graph = true;
     } else {
       if ((rc = launch_body(r, a, mode, path, st))) return rc;
     }

@@ -68,6 +68,10 @@ struct Graph {
   uint2* gedges = nullptr;  // [S]
   int* gptr = nullptr;      // [N+1]
   int2* groups = nullptr;   // [G]
+  // inbox layout: destination block b receives at most (number of groups
+  // targeting b) descriptors per step, stored from ibase[b].
+  int G = 0;
+  int* ibase = nullptr;     // [P+1]
   long long signature = 0;  // autotuner cache key
   float fanin_cv = 0.f, density = 0.f;
 };
@@ -77,15 +81,19 @@ struct Inputs {
   int B = 0, Tmax = 0;
   long long total_steps = 0, raster_words = 0;
   std::vector<int> steps_h, order_h;
-  std::vector<long long> sptr_off_h, raster_off_h;
+  std::vector<long long> sptr_off_h, raster_off_h, stepbase_h;
   int* steps = nullptr;         // [B]
   int* order = nullptr;         // [B] samples by descending step count
   long long* sptr_off = nullptr;  // [B] start of sample b's step pointers
+  long long* stepbase = nullptr;  // [B] global index of sample b's first step
   int* sched_ptr = nullptr;     // concatenated [T_b + 1] absolute entry offsets
   int* sched_nid = nullptr;     // entries sorted by neuron within a step
   float* sched_ext = nullptr;   // drive summed in event order
+  int* sched_blk = nullptr;     // [total_steps][P+1] first entry of each neuron
+                                // block per step (null when too large)
   long long* raster_off = nullptr;  // [B] first raster word of sample b
   long long n_entries = 0;
+  long long dev_bytes = 0;      // bytes copied to the device for this schedule
 };
 
 struct Run {
@@ -103,12 +111,16 @@ struct Run {
   int* err = nullptr;
   unsigned* ctl = nullptr;  // [0] barrier counter, [1] work-queue counter
   // grid-path state (one wave of Bw samples in lockstep)
-  int Bw = 0;
+  int Bw = 0, Bw_cap = 0;
   float* v = nullptr;
   int* refr = nullptr;
   float* ring = nullptr;
   int* fired = nullptr;      // [Bw][2][N]
   int* fired_cnt = nullptr;  // [Bw][2][P]
+  unsigned long long* inbox = nullptr;  // [Bw][2][G] (first edge << 32 | length)
+  int* inbox_cnt = nullptr;             // [Bw][2][P]
+  bool gplan_rsm = false;    // tier G keeps ring slices in shared memory
+  size_t gplan_smem = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.f;
   int used_mode = -1, used_path = -1;
@@ -117,6 +129,9 @@ struct Run {
   int gexec_mode = -1;
   snc_lif gexec_lif{};
   cudaStream_t gexec_stream = nullptr;
+  cudaStream_t own_stream = nullptr;  // stands in for the legacy default stream
+  bool graph_refused = false;         // stream capture failed once; launch directly
+  bool used_graph = false;            // the last launch went through the graph
 };
 
 // forward.cu

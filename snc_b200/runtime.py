@@ -59,6 +59,11 @@ def available() -> bool:
     return bool(lib().snc_b200_available())
 
 
+def set_device(device: int) -> None:
+    """Select the GPU for this thread's later calls into the library."""
+    check(lib().snc_b200_set_device(int(device)), "set_device")
+
+
 @dataclasses.dataclass
 class LIFParams:
     threshold: float = 1.0
@@ -133,6 +138,9 @@ class DeviceInputs:
         check(lib().snc_b200_inputs_upload(dg.h, ptr(ev), ev.shape[0], self.B, ptr(self.steps),
                                            C.byref(h)), "inputs_upload")
         self.h = h
+        nb, ne = C.c_int64(), C.c_int64()
+        check(lib().snc_b200_inputs_info(self.h, C.byref(nb), C.byref(ne)), "inputs_info")
+        self.device_bytes, self.entries = nb.value, ne.value
 
     def release(self):
         if getattr(self, "h", None):
@@ -165,6 +173,9 @@ class Run:
         m, p = C.c_int(), C.c_int()
         check(lib().snc_b200_run_used(self.h, C.byref(m), C.byref(p)))
         return m.value, p.value
+
+    def used_graph(self) -> bool:
+        return lib().snc_b200_run_used_graph(self.h) == 1
 
     def fetch(self, raster=False, vfinal=False) -> dict:
         B, noc, N = self.inputs.B, self.dg.n_out, self.dg.N

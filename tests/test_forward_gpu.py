@@ -28,6 +28,7 @@ def run_gpu(g, ev, steps, lif, mode, path, force_grid=False, cuda_graph=False, r
         run.launch(lif, mode=mode, path=path)
         out = run.fetch(raster=True, vfinal=True)
     out["used"] = run.used()
+    out["used_graph"] = run.used_graph()
     return out
 
 
@@ -97,6 +98,7 @@ def test_ff784_persistent_vs_oracle():
     ref = O.forward_batched(g, ev, steps, lif)
     out = run_gpu(g, ev, steps, lif, R.MODE_SORT, R.PATH_PERSISTENT, cuda_graph=True, repeat=2)
     assert_exact(out, ref)
+    assert out["used_graph"]
 
 
 def test_audio700_uneven_persistent_vs_oracle():
