@@ -191,6 +191,48 @@ int snc_b200_forward_batched(const snc_b200_graph* graph, const snc_input_event*
 int snc_b200_autotune(const snc_b200_graph* g, const snc_b200_inputs* in, const snc_lif* lif,
                       int* mode, int* path, int* block_threads);
 
+/* ---- minibatch e-prop (replaces snc::cudatrain, cuda_trainer.hpp:26-57) ----
+ * The learning rule of src/training/cuda_trainer.cu: LIF + triangular
+ * surrogate psi = gamma * max(0, 1 - |v - thr| / thr), pre trace
+ * tr = d * tr + (1 - d) * spike, eligibility E[b,s] += psi[post] * tr[pre]
+ * every step, then softmax(spike counts) - onehot(label), learning signal L
+ * (delta for OUTPUT neurons, feedback matrix . delta for INTERNAL ones) and
+ * w -= lr * mean_b(L[b,post] * E[b,s] / T_b), clamped to +-w_max.  Inputs are
+ * InputEvents (the caller encodes, as the CPU Trainer does) instead of cuRAND
+ * draws; samples of one minibatch may have different step counts. */
+typedef struct {
+  float lr;              /* TrainConfig::lr */
+  float w_max;           /* TrainConfig::w_max */
+  float surrogate_scale; /* TrainConfig::surrogate_scale (gamma) */
+  float trace_decay;     /* pre-trace decay; the reference uses lif.decay */
+  int32_t train_hidden;  /* TrainConfig::train_hidden */
+  int32_t mode;          /* delivery: SNC_B200_MODE_SORT (bit-exact) or _ATOMIC */
+} snc_eprop_cfg;
+
+typedef struct snc_b200_eprop snc_b200_eprop; /* cudatrain::CudaTrainSession */
+
+/* cudatrain::create: weights [S] (signed, CSR order) and the feedback matrix
+ * [n_internal][max(1, n_out)] (one row per INTERNAL neuron, ascending id) are
+ * supplied by the caller; max_batch bounds the samples of one minibatch. */
+int snc_b200_eprop_create(const snc_b200_graph* g, const snc_lif* lif, const snc_eprop_cfg* cfg,
+                          int32_t max_batch, const float* weights, const float* feedback,
+                          snc_b200_eprop** out);
+int snc_b200_eprop_release(snc_b200_eprop* s);                    /* cudatrain::destroy */
+int snc_b200_eprop_set_weights(snc_b200_eprop* s, const float* w); /* [S] */
+int snc_b200_eprop_get_weights(snc_b200_eprop* s, float* w);       /* [S] */
+/* One minibatch (cuda_trainer.cu run_batch, :304-350): events with sample_id
+ * in [0, B), steps [B], labels [B].  train = 0 runs the forward only (no
+ * eligibility, no update, no statistics).  counts [B][n_out] may be NULL. */
+int snc_b200_eprop_batch(snc_b200_eprop* s, const snc_input_event* events, size_t n_events,
+                         int32_t num_samples, const int32_t* steps, const int32_t* labels,
+                         int train, float* counts, snc_run_stats* stats);
+/* Eligibility [B][S] of the last training minibatch. */
+int snc_b200_eprop_get_eligibility(snc_b200_eprop* s, float* elig);
+/* cudatrain::reset_stats / collect_stats: per-synapse deliveries [S] and
+ * per-neuron firings [N] accumulated over training minibatches. */
+int snc_b200_eprop_reset_stats(snc_b200_eprop* s);
+int snc_b200_eprop_collect_stats(snc_b200_eprop* s, int64_t* syn_deliveries, int64_t* neuron_fires);
+
 #ifdef __cplusplus
 }
 #endif

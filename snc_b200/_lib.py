@@ -67,6 +67,14 @@ SIGNATURES = {
     "snc_b200_forward": (C.c_int, [P, P, P, C.c_size_t, I32, P, C.c_int, P, P]),
     "snc_b200_forward_batched": (C.c_int, [P, P, C.c_size_t, I32, P, P, C.c_int, P, P, P, P]),
     "snc_b200_autotune": (C.c_int, [P, P, P, P, P, P]),
+    "snc_b200_eprop_create": (C.c_int, [P, P, P, I32, P, P, P]),
+    "snc_b200_eprop_release": (C.c_int, [P]),
+    "snc_b200_eprop_set_weights": (C.c_int, [P, P]),
+    "snc_b200_eprop_get_weights": (C.c_int, [P, P]),
+    "snc_b200_eprop_batch": (C.c_int, [P, P, C.c_size_t, I32, P, P, C.c_int, P, P]),
+    "snc_b200_eprop_get_eligibility": (C.c_int, [P, P]),
+    "snc_b200_eprop_reset_stats": (C.c_int, [P]),
+    "snc_b200_eprop_collect_stats": (C.c_int, [P, P, P]),
 }
 
 _LIB = None

@@ -12,10 +12,6 @@
 
 #include "internal.h"
 
-struct snc_b200_graph : sncb::Graph {};
-struct snc_b200_inputs : sncb::Inputs {};
-struct snc_b200_run : sncb::Run {};
-
 namespace sncb {
 
 static thread_local std::string g_last_error;
@@ -215,7 +211,7 @@ static int upload_graph(const snc_graph_view* v, Graph* g) {
 // build_schedule (cpu_backend.cpp:43-65) for a batch: per (sample, step) the
 // (neuron, drive) entries sorted by neuron, each drive summed from 0.0f in
 // event order (cpu_backend.cpp:99).  ignore_sample maps every event to sample 0.
-static int upload_inputs(const Graph* g, const snc_input_event* ev, size_t n_ev, int B,
+int upload_inputs(const Graph* g, const snc_input_event* ev, size_t n_ev, int B,
                          const int32_t* steps, bool ignore_sample, Inputs* in) {
   if (B < 0 || (B > 0 && !steps) || (n_ev > 0 && !ev)) {
     set_error("bad inputs arguments");
@@ -331,7 +327,7 @@ static int upload_inputs(const Graph* g, const snc_input_event* ev, size_t n_ev,
   return SNC_B200_OK;
 }
 
-static void free_inputs(Inputs* in) {
+void free_inputs(Inputs* in) {
   if (!in) return;
   for (void* p : {(void*)in->steps, (void*)in->order, (void*)in->sptr_off, (void*)in->sched_ptr,
                   (void*)in->sched_nid, (void*)in->sched_ext, (void*)in->raster_off,
@@ -465,8 +461,9 @@ const char* snc_b200_last_error(void) { return g_last_error.c_str(); }
 int snc_b200_graph_upload(const snc_graph_view* v, snc_b200_graph** out) {
   if (!out) { set_error("null out"); return SNC_B200_EINVAL; }
   *out = nullptr;
-  int rc = check_device();
+  int rc = validate_view(v);
   if (rc) return rc;
+  if ((rc = check_device())) return rc;
   auto* g = new snc_b200_graph();
   rc = upload_graph(v, g);
   if (rc) { free_graph(g); delete g; return rc; }

@@ -1,0 +1,345 @@
+// Minibatch e-prop (the cudatrain:: session of the reference, re-designed):
+// the forward with surrogate / trace / eligibility runs in the
+// sample-per-CTA persistent kernel (forward.cu, k_tier_s<.., true>), the
+// update in three small kernels below.
+//
+// Reference: src/training/cuda_trainer.cu
+//   k_softmax_delta   :131-142   softmax(counts) - onehot(label)
+//   k_learning_signal :144-161   L = delta (OUTPUT) / B . delta (INTERNAL)
+//   k_apply           :163-172   w -= lr/T * (sum_b L*E) / bs, clamp
+// Every floating-point operation is written out (__fmul_rn / __fadd_rn) in
+// the order of the CPU restatement, so results match it up to the expf of the
+// softmax.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "device_common.cuh"
+#include "internal.h"
+
+struct snc_b200_eprop {
+  const sncb::Graph* g = nullptr;
+  snc_lif lif{};
+  snc_eprop_cfg cfg{};
+  int max_batch = 0, n_internal = 0, oc = 1;
+  uint2* edges = nullptr;                // trainer weights, CSR order
+  float* bmat = nullptr;                 // [n_internal][oc]
+  int* internal_row = nullptr;           // [N]
+  float* elig = nullptr;                 // [max_batch][S]
+  int* counts = nullptr;                 // [max_batch][oc]
+  float* delta = nullptr;                // [max_batch][oc]
+  float* L = nullptr;                    // [max_batch][N]
+  int* labels = nullptr;                 // [max_batch]
+  int* steps = nullptr;                  // [max_batch]
+  unsigned long long* spikes = nullptr;  // [max_batch]
+  unsigned long long* events = nullptr;  // [max_batch]
+  unsigned long long* fires = nullptr;   // [N]
+  int* err = nullptr;
+  unsigned* ctl = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int last_B = 0;
+  bool have_elig = false;
+};
+
+namespace sncb {
+
+__global__ void k_softmax_delta(int B, int oc, const int* counts, const int* labels, float* delta) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  const int* c = counts + (size_t)b * oc;
+  float mx = (float)c[0];
+  for (int k = 1; k < oc; ++k) mx = fmaxf(mx, (float)c[k]);
+  float sum = 0.f;
+  for (int k = 0; k < oc; ++k) sum = __fadd_rn(sum, expf(__fsub_rn((float)c[k], mx)));
+  for (int k = 0; k < oc; ++k)
+    delta[(size_t)b * oc + k] = __fsub_rn(__fdiv_rn(expf(__fsub_rn((float)c[k], mx)), sum),
+                                          k == labels[b] ? 1.f : 0.f);
+}
+
+__global__ void k_learning_signal(int B, int N, int oc, int train_hidden, const uint8_t* role,
+                                  const int* channel, const int* internal_row, const float* bmat,
+                                  const float* delta, float* L) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (long long)B * N) return;
+  const int b = (int)(tid / N), j = (int)(tid % N);
+  float lv = 0.f;
+  if (role[j] == 2 && channel[j] >= 0 && channel[j] < oc) {
+    lv = delta[(size_t)b * oc + channel[j]];
+  } else if (train_hidden && internal_row[j] >= 0) {
+    const float* br = bmat + (size_t)internal_row[j] * oc;
+    float s = 0.f;
+    for (int k = 0; k < oc; ++k) s = __fadd_rn(s, __fmul_rn(br[k], delta[(size_t)b * oc + k]));
+    lv = s;
+  }
+  L[tid] = lv;
+}
+
+__global__ void k_apply(int S, int N, int B, int uniform, float lr, float lr_over_T, float w_max,
+                        const int* post, const int* steps, const float* L, const float* E,
+                        uint2* edges) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S) return;
+  const int p = post[s];
+  float acc = 0.f;
+  float nw;
+  const float w = __uint_as_float(edges[s].y);
+  if (uniform) {
+    for (int b = 0; b < B; ++b)
+      acc = __fadd_rn(acc, __fmul_rn(L[(size_t)b * N + p], E[(size_t)b * S + s]));
+    nw = __fsub_rn(w, __fdiv_rn(__fmul_rn(lr_over_T, acc), (float)B));
+  } else {
+    for (int b = 0; b < B; ++b)
+      acc = __fadd_rn(acc, __fdiv_rn(__fmul_rn(L[(size_t)b * N + p], E[(size_t)b * S + s]),
+                                     (float)max(1, steps[b])));
+    nw = __fsub_rn(w, __fdiv_rn(__fmul_rn(lr, acc), (float)B));
+  }
+  nw = fminf(fmaxf(nw, -w_max), w_max);
+  edges[s].y = __float_as_uint(nw);
+}
+
+__global__ void k_set_weights(int S, const float* w, uint2* edges) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < S) edges[s].y = __float_as_uint(w[s]);
+}
+
+__global__ void k_get_weights(int S, const uint2* edges, float* w) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < S) w[s] = __uint_as_float(edges[s].y);
+}
+
+static inline int grid_of(long long n, int b = 256) { return (int)std::max(1ll, (n + b - 1) / b); }
+
+static void free_session(snc_b200_eprop* s) {
+  for (void* p : {(void*)s->edges, (void*)s->bmat, (void*)s->internal_row, (void*)s->elig,
+                  (void*)s->counts, (void*)s->delta, (void*)s->L, (void*)s->labels,
+                  (void*)s->steps, (void*)s->spikes, (void*)s->events, (void*)s->fires,
+                  (void*)s->err, (void*)s->ctl})
+    dev_free(p);
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+}
+
+static int create_session(snc_b200_eprop* s, const Graph* g, const snc_lif* lif,
+                          const snc_eprop_cfg* cfg, int max_batch, const float* w,
+                          const float* feedback) {
+  s->g = g;
+  s->lif = *lif;
+  s->cfg = *cfg;
+  s->max_batch = max_batch;
+  s->oc = std::max(1, g->noc);
+  const int N = g->N, S = g->S;
+  std::vector<uint8_t> role(N);
+  SNCB_CUDA(cudaMemcpy(role.data(), g->role, N, cudaMemcpyDeviceToHost));
+  std::vector<int> irow(N, -1);
+  for (int i = 0; i < N; ++i)
+    if (role[i] == 0) irow[i] = s->n_internal++;
+  // trainer edges: the graph's packed edges with the trainer's weights
+  std::vector<uint2> edges((size_t)S + 2);
+  SNCB_CUDA(cudaMemcpy(edges.data(), g->edges, ((size_t)S + 2) * sizeof(uint2), cudaMemcpyDeviceToHost));
+  for (int e = 0; e < S; ++e) std::memcpy(&edges[e].y, &w[e], 4);
+  int rc;
+  if ((rc = dev_upload(&s->edges, edges.data(), edges.size()))) return rc;
+  if ((rc = dev_upload(&s->bmat, feedback, (size_t)std::max(1, s->n_internal) * s->oc))) return rc;
+  if ((rc = dev_upload(&s->internal_row, irow.data(), (size_t)N))) return rc;
+  const size_t B = (size_t)max_batch;
+  if ((rc = dev_alloc(&s->elig, B * std::max(1, S)))) return rc;
+  if ((rc = dev_alloc(&s->counts, B * s->oc))) return rc;
+  if ((rc = dev_alloc(&s->delta, B * s->oc))) return rc;
+  if ((rc = dev_alloc(&s->L, B * std::max(1, N)))) return rc;
+  if ((rc = dev_alloc(&s->labels, B))) return rc;
+  if ((rc = dev_alloc(&s->steps, B))) return rc;
+  if ((rc = dev_alloc(&s->spikes, B))) return rc;
+  if ((rc = dev_alloc(&s->events, B))) return rc;
+  if ((rc = dev_alloc(&s->fires, (size_t)std::max(1, N)))) return rc;
+  if ((rc = dev_alloc(&s->err, 1))) return rc;
+  if ((rc = dev_alloc(&s->ctl, 4))) return rc;
+  SNCB_CUDA(cudaMemset(s->fires, 0, (size_t)std::max(1, N) * sizeof(unsigned long long)));
+  SNCB_CUDA(cudaEventCreate(&s->ev0));
+  SNCB_CUDA(cudaEventCreate(&s->ev1));
+  return SNC_B200_OK;
+}
+
+static int run_batch(snc_b200_eprop* s, const snc_input_event* ev, size_t n_ev, int B,
+                     const int32_t* steps, const int32_t* labels, int train, float* counts_out,
+                     snc_run_stats* stats) {
+  const Graph* g = s->g;
+  if (B < 1 || B > s->max_batch || !steps || (train && !labels)) {
+    set_error("e-prop batch: bad sample count, steps or labels");
+    return SNC_B200_EINVAL;
+  }
+  Inputs in;
+  int rc = upload_inputs(g, ev, n_ev, B, steps, false, &in);
+  if (rc) { free_inputs(&in); return rc; }
+  cudaStream_t st = nullptr;
+  const int oc = s->oc, N = g->N, S = g->S;
+  bool ok = true;
+  auto chk = [&](cudaError_t e, const char* what) {
+    if (ok && e != cudaSuccess) { rc = cuda_fail(e, what); ok = false; }
+  };
+  chk(cudaMemsetAsync(s->counts, 0, (size_t)B * oc * sizeof(int), st), "memset counts");
+  chk(cudaMemsetAsync(s->spikes, 0, (size_t)B * 8, st), "memset spikes");
+  chk(cudaMemsetAsync(s->events, 0, (size_t)B * 8, st), "memset events");
+  chk(cudaMemsetAsync(s->ctl, 0, 16, st), "memset ctl");
+  chk(cudaMemsetAsync(s->err, 0, 4, st), "memset err");
+  if (train) chk(cudaMemsetAsync(s->elig, 0, (size_t)B * S * sizeof(float), st), "memset elig");
+  if (train) {
+    chk(cudaMemcpyAsync(s->labels, labels, (size_t)B * 4, cudaMemcpyHostToDevice, st), "labels");
+    chk(cudaMemcpyAsync(s->steps, steps, (size_t)B * 4, cudaMemcpyHostToDevice, st), "steps");
+  }
+  chk(cudaEventRecord(s->ev0, st), "event");
+  if (ok) {
+    EpropLaunch e;
+    e.g = g;
+    e.in = &in;
+    e.edges = s->edges;
+    e.counts = s->counts;
+    e.spikes = s->spikes;
+    e.events = s->events;
+    e.elig = train ? s->elig : nullptr;
+    e.fires = train ? s->fires : nullptr;
+    e.gamma = s->cfg.surrogate_scale;
+    e.trace_decay = s->cfg.trace_decay;
+    e.lif = s->lif;
+    e.mode = s->cfg.mode == SNC_B200_MODE_SORT ? SNC_B200_MODE_SORT : SNC_B200_MODE_ATOMIC;
+    e.err = s->err;
+    e.ctl = s->ctl;
+    rc = launch_eprop_forward(e, st);
+    ok = rc == SNC_B200_OK;
+  }
+  if (ok && train) {
+    bool uniform = true;
+    for (int b = 1; b < B; ++b) uniform = uniform && steps[b] == steps[0];
+    const float lr_over_T = s->cfg.lr / (float)std::max(1, steps[0]);
+    k_softmax_delta<<<grid_of(B), 256, 0, st>>>(B, oc, s->counts, s->labels, s->delta);
+    k_learning_signal<<<grid_of((long long)B * N), 256, 0, st>>>(
+        B, N, oc, s->cfg.train_hidden, g->role, g->channel, s->internal_row, s->bmat, s->delta, s->L);
+    k_apply<<<grid_of(S), 256, 0, st>>>(S, N, B, uniform ? 1 : 0, s->cfg.lr, lr_over_T,
+                                        s->cfg.w_max, g->post, s->steps, s->L, s->elig, s->edges);
+    chk(cudaGetLastError(), "e-prop update kernels");
+  }
+  chk(cudaEventRecord(s->ev1, st), "event");
+  chk(cudaEventSynchronize(s->ev1), "synchronize");
+  if (ok) {
+    std::vector<int> cnt((size_t)B * oc);
+    std::vector<unsigned long long> sp(B), en(B);
+    chk(cudaMemcpy(cnt.data(), s->counts, cnt.size() * 4, cudaMemcpyDeviceToHost), "counts");
+    chk(cudaMemcpy(sp.data(), s->spikes, (size_t)B * 8, cudaMemcpyDeviceToHost), "spikes");
+    chk(cudaMemcpy(en.data(), s->events, (size_t)B * 8, cudaMemcpyDeviceToHost), "events");
+    int err = 0;
+    chk(cudaMemcpy(&err, s->err, 4, cudaMemcpyDeviceToHost), "err");
+    if (ok && counts_out)
+      for (int b = 0; b < B; ++b)
+        for (int c = 0; c < g->noc; ++c) counts_out[(size_t)b * g->noc + c] = (float)cnt[(size_t)b * oc + c];
+    if (ok && stats) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+      stats->spikes = stats->synaptic_events = 0;
+      for (int b = 0; b < B; ++b) {
+        stats->spikes += (long long)sp[b];
+        stats->synaptic_events += (long long)en[b];
+      }
+      stats->overflow = 0;
+      stats->ms = ms;
+    }
+    if (ok && err) {
+      set_error("device error word set");
+      rc = err;
+      ok = false;
+    }
+  }
+  s->last_B = B;
+  s->have_elig = ok && train;
+  free_inputs(&in);
+  return rc;
+}
+
+}  // namespace sncb
+
+using namespace sncb;
+
+extern "C" {
+
+int snc_b200_eprop_create(const snc_b200_graph* g, const snc_lif* lif, const snc_eprop_cfg* cfg,
+                          int32_t max_batch, const float* weights, const float* feedback,
+                          snc_b200_eprop** out) {
+  if (!g || !lif || !cfg || !weights || !out || max_batch < 1) {
+    set_error("e-prop create: bad argument");
+    return SNC_B200_EINVAL;
+  }
+  *out = nullptr;
+  auto* s = new snc_b200_eprop();
+  int rc = create_session(s, static_cast<const Graph*>(g), lif, cfg, max_batch, weights, feedback);
+  if (rc) { free_session(s); delete s; return rc; }
+  *out = s;
+  return SNC_B200_OK;
+}
+
+int snc_b200_eprop_release(snc_b200_eprop* s) {
+  if (!s) return SNC_B200_OK;
+  free_session(s);
+  delete s;
+  return SNC_B200_OK;
+}
+
+int snc_b200_eprop_set_weights(snc_b200_eprop* s, const float* w) {
+  if (!s || !w) { set_error("null argument"); return SNC_B200_EINVAL; }
+  float* d = nullptr;
+  int rc = dev_upload(&d, w, (size_t)std::max(1, s->g->S));
+  if (rc) return rc;
+  k_set_weights<<<grid_of(s->g->S), 256>>>(s->g->S, d, s->edges);
+  cudaError_t e = cudaDeviceSynchronize();
+  dev_free(d);
+  if (e != cudaSuccess) return cuda_fail(e, "set_weights");
+  return SNC_B200_OK;
+}
+
+int snc_b200_eprop_get_weights(snc_b200_eprop* s, float* w) {
+  if (!s || !w) { set_error("null argument"); return SNC_B200_EINVAL; }
+  float* d = nullptr;
+  int rc = dev_alloc(&d, (size_t)std::max(1, s->g->S));
+  if (rc) return rc;
+  k_get_weights<<<grid_of(s->g->S), 256>>>(s->g->S, s->edges, d);
+  cudaError_t e = cudaMemcpy(w, d, (size_t)s->g->S * sizeof(float), cudaMemcpyDeviceToHost);
+  dev_free(d);
+  if (e != cudaSuccess) return cuda_fail(e, "get_weights");
+  return SNC_B200_OK;
+}
+
+int snc_b200_eprop_batch(snc_b200_eprop* s, const snc_input_event* events, size_t n_events,
+                         int32_t num_samples, const int32_t* steps, const int32_t* labels,
+                         int train, float* counts, snc_run_stats* stats) {
+  if (!s) { set_error("null session"); return SNC_B200_EINVAL; }
+  return run_batch(s, events, n_events, num_samples, steps, labels, train, counts, stats);
+}
+
+int snc_b200_eprop_get_eligibility(snc_b200_eprop* s, float* elig) {
+  if (!s || !elig) { set_error("null argument"); return SNC_B200_EINVAL; }
+  if (!s->have_elig) { set_error("no training minibatch has run"); return SNC_B200_EINVAL; }
+  SNCB_CUDA(cudaMemcpy(elig, s->elig, (size_t)s->last_B * s->g->S * sizeof(float), cudaMemcpyDeviceToHost));
+  return SNC_B200_OK;
+}
+
+int snc_b200_eprop_reset_stats(snc_b200_eprop* s) {
+  if (!s) { set_error("null session"); return SNC_B200_EINVAL; }
+  SNCB_CUDA(cudaMemset(s->fires, 0, (size_t)std::max(1, s->g->N) * sizeof(unsigned long long)));
+  return SNC_B200_OK;
+}
+
+// Every spike of neuron i delivers each of its outgoing synapses once
+// (cuda_trainer.cu:182-185), so a synapse's delivery count is its pre
+// neuron's firing count.
+int snc_b200_eprop_collect_stats(snc_b200_eprop* s, int64_t* syn_deliveries, int64_t* neuron_fires) {
+  if (!s) { set_error("null session"); return SNC_B200_EINVAL; }
+  const Graph* g = s->g;
+  std::vector<unsigned long long> f((size_t)std::max(1, g->N));
+  SNCB_CUDA(cudaMemcpy(f.data(), s->fires, (size_t)g->N * 8, cudaMemcpyDeviceToHost));
+  if (neuron_fires)
+    for (int i = 0; i < g->N; ++i) neuron_fires[i] = (int64_t)f[i];
+  if (syn_deliveries)
+    for (int i = 0; i < g->N; ++i)
+      for (int e = g->row_ptr_h[i]; e < g->row_ptr_h[i + 1]; ++e) syn_deliveries[e] = (int64_t)f[i];
+  return SNC_B200_OK;
+}
+
+}  // extern "C"

@@ -93,6 +93,10 @@ struct FwdArgs {
   int* err;
   unsigned* ctl;
   LifP lif;
+  // e-prop (tier S only): eligibility [B][S], per-neuron fire counts
+  float* elig;
+  unsigned long long* fires;
+  float gamma, trace_decay;
 };
 
 // Shared-memory bytes of the tier-S kernel for this graph.
@@ -110,13 +114,16 @@ int tier_s_smem_bytes(const Graph* g, int mode, bool eprop) {
 // ---------------------------------------------------------------------------
 // one LIF neuron (cpu_backend.cpp:129-143, plus reset_mode 1 = subtractive)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int lif_step(const LifP& p, float& v, int& refr, float ext, float rin) {
+__device__ __forceinline__ int lif_step(const LifP& p, float& v, int& refr, float ext, float rin,
+                                        float* vpre = nullptr) {
   if (refr > 0) {
     --refr;
     v = p.reset;
+    if (vpre) *vpre = p.reset;
     return 0;
   }
   const float nv = lif_integrate(v, p.decay, ext, rin);
+  if (vpre) *vpre = nv;
   if (nv >= p.thr) {
     v = p.reset_mode ? __fsub_rn(nv, p.thr) : p.reset;
     refr = p.refractory;
@@ -247,7 +254,7 @@ __device__ void apply_ordered(int ce, int* head, int* tail, int ncols_local, con
 // ---------------------------------------------------------------------------
 // tier S: one CTA per sample, state in shared memory
 // ---------------------------------------------------------------------------
-template <int MODE>
+template <int MODE, bool EP>
 __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int scratch[40];
@@ -270,6 +277,10 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
   int* st_slot = st_col + CH;
   float* st_w = reinterpret_cast<float*>(st_slot + CH);
   int* st_next = reinterpret_cast<int*>(st_w + CH);
+  // e-prop: pre-synaptic trace per neuron, surrogate psi per ring column
+  float* tr = MODE == MODE_SORT ? reinterpret_cast<float*>(st_next + CH)
+                                : reinterpret_cast<float*>(counts + noc);
+  float* psi = tr + N;
 
   for (;;) {
     if (tid == 0) s_q = (int)atomicAdd(&a.ctl[1], 1u);
@@ -283,6 +294,7 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
       v[i] = 0.f;
       refr[i] = 0;
       ext[i] = 0.f;
+      if (EP) tr[i] = 0.f;
     }
     for (int i = tid; i < noc; i += nthr) counts[i] = 0;
     if (MODE == MODE_SORT)
@@ -315,9 +327,19 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
             rin = slot[c];
             slot[c] = 0.f;
           }
-          f = lif_step(a.lif, vv, rr, e, rin);
+          float vpre;
+          f = lif_step(a.lif, vv, rr, e, rin, &vpre);
           v[j] = vv;
           refr[j] = rr;
+          if (EP) {
+            // cuda_trainer.cu:151-153: triangular surrogate and pre trace
+            const float thr = a.lif.thr;
+            const float dd = __fdiv_rn(fabsf(__fsub_rn(vpre, thr)), thr > 0.f ? thr : 1.f);
+            if (c >= 0) psi[c] = dd < 1.f ? __fmul_rn(a.gamma, __fsub_rn(1.f, dd)) : 0.f;
+            tr[j] = __fadd_rn(__fmul_rn(a.trace_decay, tr[j]),
+                              __fmul_rn(__fsub_rn(1.f, a.trace_decay), f ? 1.f : 0.f));
+            if (f && a.fires) atomicAdd(&a.fires[j], 1ull);
+          }
           if (f) {
             ++my_spikes;
             my_events += a.row_ptr[j + 1] - a.row_ptr[j];
@@ -334,6 +356,20 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
         nf += tot;
       }
       __syncthreads();
+      if (EP && a.elig) {
+        // cuda_trainer.cu:105-112: E[b,s] += psi[post] * tr[pre]; rows whose
+        // trace is exactly zero add +0 and are skipped (trainer.cpp:243-244)
+        float* Eb = a.elig + (size_t)b * a.S;
+        for (int i = warp; i < N; i += nwarps) {
+          const float tri = tr[i];
+          if (tri == 0.f) continue;
+          const int rs = a.row_ptr[i], re = a.row_ptr[i + 1];
+          for (int e = rs + lane; e < re; e += 32) {
+            const uint2 ed = a.edges[e];
+            Eb[e] = __fadd_rn(Eb[e], __fmul_rn(psi[edge_col(ed)], tri));
+          }
+        }
+      }
       if (MODE != MODE_SORT) {
         // warp per fired row; two edges per lane per 128-bit load
         for (int k = warp; k < nf; k += nwarps) {
@@ -933,22 +969,52 @@ static int optin_smem() {
   return optin;
 }
 
-template <int MODE>
-static int launch_tier_s(Run* r, const FwdArgs& a, cudaStream_t st) {
-  const Graph* g = r->g;
+template <int MODE, bool EP>
+static int launch_tier_s_kernel(const Graph* g, int B, const FwdArgs& a, cudaStream_t st) {
   const int nthr = 1024;
-  const size_t smem = tier_s_bytes(g->N, g->ncols, g->R, a.noc, MODE, false, nthr);
-  SNCB_CUDA(cudaFuncSetAttribute(k_tier_s<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const size_t smem = tier_s_bytes(g->N, g->ncols, g->R, a.noc, MODE, EP, nthr);
+  SNCB_CUDA(cudaFuncSetAttribute(k_tier_s<MODE, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  SNCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tier_s<MODE>, nthr, smem));
+  SNCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tier_s<MODE, EP>, nthr, smem));
   if (per_sm < 1) {
     set_error("tier S does not fit on an SM");
     return SNC_B200_EUNSUPPORTED;
   }
-  const int grid = std::max(1, std::min(r->in->B, per_sm * g->sm_count));
-  k_tier_s<MODE><<<grid, nthr, smem, st>>>(a);
+  const int grid = std::max(1, std::min(B, per_sm * g->sm_count));
+  k_tier_s<MODE, EP><<<grid, nthr, smem, st>>>(a);
   SNCB_CUDA(cudaGetLastError());
   return SNC_B200_OK;
+}
+
+template <int MODE>
+static int launch_tier_s(Run* r, const FwdArgs& a, cudaStream_t st) {
+  return launch_tier_s_kernel<MODE, false>(r->g, r->in->B, a, st);
+}
+
+// e-prop forward of one minibatch (tier S with eligibility), see eprop.cu.
+int launch_eprop_forward(const EpropLaunch& e, cudaStream_t st) {
+  const Graph* g = e.g;
+  const Inputs* in = e.in;
+  if (tier_s_bytes(g->N, g->ncols, g->R, std::max(1, g->noc), e.mode, true, 1024) >
+      (size_t)optin_smem()) {
+    set_error("e-prop: one sample's state does not fit in one CTA's shared memory");
+    return SNC_B200_EUNSUPPORTED;
+  }
+  FwdArgs a{};
+  a.N = g->N; a.S = g->S; a.R = g->R; a.ncols = g->ncols; a.noc = std::max(1, g->noc);
+  a.P = g->P; a.BS = g->BS; a.G = g->G;
+  a.row_ptr = g->row_ptr; a.edges = e.edges; a.gedges = g->gedges; a.col_of = g->col_of;
+  a.out_ch = g->out_ch;
+  a.B = in->B; a.order = in->order; a.steps = in->steps; a.sptr_off = in->sptr_off;
+  a.stepbase = in->stepbase; a.sched_ptr = in->sched_ptr; a.sched_nid = in->sched_nid;
+  a.sched_ext = in->sched_ext; a.raster_off = in->raster_off;
+  a.counts = e.counts; a.spikes = e.spikes; a.events = e.events;
+  a.W = (g->N + 31) / 32;
+  a.err = e.err; a.ctl = e.ctl;
+  a.lif = LifP{e.lif.threshold, e.lif.decay, e.lif.reset, e.lif.refractory, e.lif.reset_mode};
+  a.elig = e.elig; a.fires = e.fires; a.gamma = e.gamma; a.trace_decay = e.trace_decay;
+  if (e.mode == MODE_SORT) return launch_tier_s_kernel<MODE_SORT, true>(g, in->B, a, st);
+  return launch_tier_s_kernel<MODE_ATOMIC, true>(g, in->B, a, st);
 }
 
 // Wave size and ring placement of the tier-G kernel for this run.

@@ -134,9 +134,38 @@ struct Run {
   bool used_graph = false;            // the last launch went through the graph
 };
 
+// One e-prop minibatch forward (tier S kernel with eligibility).
+struct EpropLaunch {
+  const Graph* g = nullptr;
+  const Inputs* in = nullptr;
+  const uint2* edges = nullptr;  // packed edges carrying the trainer's weights
+  int* counts = nullptr;         // [B][max(1,noc)]
+  unsigned long long* spikes = nullptr;
+  unsigned long long* events = nullptr;
+  float* elig = nullptr;         // [B][S] (null: no eligibility)
+  unsigned long long* fires = nullptr;
+  float gamma = 0.f, trace_decay = 0.f;
+  snc_lif lif{};
+  int mode = 2;
+  int* err = nullptr;
+  unsigned* ctl = nullptr;
+};
+
+// api.cu: the per-step injection schedule of a batch (build_schedule,
+// cpu_backend.cpp:43-65); ignore_sample maps every event to sample 0.
+int upload_inputs(const Graph* g, const snc_input_event* ev, size_t n_ev, int B,
+                  const int32_t* steps, bool ignore_sample, Inputs* in);
+void free_inputs(Inputs* in);
+
 // forward.cu
+int launch_eprop_forward(const EpropLaunch& e, cudaStream_t stream);
 int launch_run(Run* r, const snc_lif* lif, int mode, int path, cudaStream_t stream);
 int tier_s_smem_bytes(const Graph* g, int mode, bool eprop);
 int resolve_auto(const Graph* g, const Inputs* in, int* mode, int* path);
 
 }  // namespace sncb
+
+// The opaque handles of the C ABI.
+struct snc_b200_graph : sncb::Graph {};
+struct snc_b200_inputs : sncb::Inputs {};
+struct snc_b200_run : sncb::Run {};
