@@ -191,6 +191,111 @@ def cpu_baseline(g, ev, lif, budget_s=10.0):
             "sample": f"{n} full rec100k forwards (1000 steps, batch 1), serial cpu backend"}
 
 
+def _time_cuda(fn, steps, warmup):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(steps):
+        fn()
+    t1.record()
+    torch.cuda.synchronize()
+    return t0.elapsed_time(t1) / steps
+
+
+def bptt_leg(steps=3, warmup=2, lm=True):
+    """BPTT step (forward + backward) of the custom kernels against the
+    PyTorch-autograd bridge (oracle/bptt_ref.py, the reference bridge's model
+    with per-synapse delays) on the same GPU.
+      mnist-like: 784 Poisson -> 512 -> 512 LIF (local sparse, delays 1-4)
+                  -> 10 leaky readout, T=100, B=128, checkpoint every 10.
+      char-LM:    4096 recurrent LIF, fan-in 64, delays 1-8, 96-symbol
+                  Zipf tokens, B=64, T=256, checkpoint every 16."""
+    import torch
+    import torch.nn.functional as F
+
+    from oracle import bptt_ref as BR
+    from snc_b200 import bptt as BP
+    from snc_b200 import workloads as W
+    out = {}
+    c4 = W.bptt_mnist_like()
+    dev = "cuda"
+    model = BP.DelayedSNN(c4["N"], c4["pre"], c4["post"], c4["delays"], c4["n_in"],
+                          c4["readout_ids"], 10, thr=1.0, decay=0.95, surrogate_scale=25.0,
+                          ckpt_every=10).to(dev)
+    x = torch.as_tensor(c4["spikes"], device=dev)
+    y = torch.as_tensor(c4["labels"], device=dev)
+
+    def custom():
+        model.zero_grad(set_to_none=True)
+        F.cross_entropy(model(x), y).backward()
+
+    order = np.argsort(c4["pre"], kind="stable")
+    w_ref = model.w.detach().clone().requires_grad_(True)
+    wro = model.readout.weight.detach().clone().requires_grad_(True)
+    bro = model.readout.bias.detach().clone().requires_grad_(True)
+    pre = torch.as_tensor(c4["pre"], device=dev).long()
+    post = torch.as_tensor(c4["post"], device=dev).long()
+    dl = torch.as_tensor(c4["delays"], device=dev).long()
+    rid = torch.as_tensor(c4["readout_ids"], device=dev).long()
+
+    def reference():
+        for p in (w_ref, wro, bro):
+            p.grad = None
+        ext = torch.zeros(x.shape[0], x.shape[1], c4["N"], device=dev)
+        ext[:, :, :c4["n_in"]] = x
+        s = BR.core_forward(w_ref, ext, pre, post, dl, 1.0, 0.95, 25.0)
+        F.cross_entropy(BR.leaky_readout(s, wro, bro, rid, 0.9), y).backward()
+
+    del order
+    ms_c = _time_cuda(custom, steps, warmup)
+    ms_r = _time_cuda(reference, steps, warmup)
+    rel = float((model.w.grad - w_ref.grad).abs().max() / w_ref.grad.abs().max().clamp_min(1e-30))
+    out["mnist_like"] = {"custom_ms": ms_c, "autograd_ms": ms_r, "speedup": ms_r / ms_c,
+                         "grad_rel_err": rel, "T": 100, "B": 128, "synapses": int(len(c4["pre"]))}
+    if lm:
+        c5 = W.char_lm()
+        torch.manual_seed(0)
+        net = BP.SpikingLM(c5["vocab"], c5["H"], c5["pre"], c5["post"], c5["delays"], w_scale=2.0,
+                           ckpt_every=16).to(dev)
+        xt = torch.as_tensor(c5["x"], device=dev)
+        yt = torch.as_tensor(c5["y"], device=dev)
+
+        def lm_custom():
+            net.zero_grad(set_to_none=True)
+            F.cross_entropy(net(xt).reshape(-1, c5["vocab"]), yt.reshape(-1)).backward()
+
+        pre5 = torch.as_tensor(c5["pre"], device=dev).long()
+        post5 = torch.as_tensor(c5["post"], device=dev).long()
+        d5 = torch.as_tensor(c5["delays"], device=dev).long()
+        emb = net.embed.weight.detach().clone().requires_grad_(True)
+        wr = net.w_rec.detach().clone().requires_grad_(True)
+        wo = net.readout.weight.detach().clone().requires_grad_(True)
+        bo = net.readout.bias.detach().clone().requires_grad_(True)
+
+        def lm_reference():
+            for p in (emb, wr, wo, bo):
+                p.grad = None
+            s = BR.core_forward(wr, emb[xt].transpose(0, 1), pre5, post5, d5, 1.0, 0.95, 25.0)
+            r = torch.zeros(xt.shape[0], c5["H"], device=dev)
+            rs = []
+            for t in range(s.shape[0]):
+                r = 0.9 * r + s[t]
+                rs.append(r)
+            lg = F.linear(torch.stack(rs, 1), wo, bo)
+            F.cross_entropy(lg.reshape(-1, c5["vocab"]), yt.reshape(-1)).backward()
+
+        ms_c5 = _time_cuda(lm_custom, 2, 1)
+        ms_r5 = _time_cuda(lm_reference, 1, 1)
+        rel5 = float((net.w_rec.grad - wr.grad).abs().max() / wr.grad.abs().max().clamp_min(1e-30))
+        out["char_lm"] = {"custom_ms": ms_c5, "autograd_ms": ms_r5, "speedup": ms_r5 / ms_c5,
+                          "grad_rel_err": rel5, "T": 256, "B": 64, "synapses": int(len(c5["pre"])),
+                          "tokens_per_s": 64 * 256 / (ms_c5 / 1e3)}
+    return out
+
+
 def our_arm(args):
     import torch
     rank, world, local = dist_setup()
@@ -303,6 +408,7 @@ def our_arm(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_extra:
         cpu = cpu_baseline(g, ev, lif)
+        extra["bptt"] = bptt_leg()
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,

@@ -233,6 +233,36 @@ int snc_b200_eprop_get_eligibility(snc_b200_eprop* s, float* elig);
 int snc_b200_eprop_reset_stats(snc_b200_eprop* s);
 int snc_b200_eprop_collect_stats(snc_b200_eprop* s, int64_t* syn_deliveries, int64_t* neuron_fires);
 
+/* ---- surrogate-gradient BPTT (replaces the autograd unrolling of the bridge,
+ * python/snc/model.py:52-72, with the per-synapse delays of
+ * python/snc/shd_model.py:109-121) -------------------------------------------
+ * Graph: CSR over outgoing synapses (row_ptr [N+1], post [S], delays [S]).
+ * All tensors are DEVICE pointers, batch innermost: ext / spikes / grads are
+ * [T][N][B] fp32, weights [S] in CSR order.  Calls are ordered on `stream`
+ * (a cudaStream_t) and return after it has drained; one handle must not be
+ * used from two streams at once (it owns the workspaces).
+ *   forward:  v = decay*v + sum_e w_e s_pre(t - d_e) + ext; s = H(v - thr)
+ *             (smooth != 0: s = x / (1 + slope |x|)); v = v * (1 - s).
+ *             Saves spike_bits [T][N][ceil(B/32)] and v_saved: with
+ *             ckpt_every = K > 0, v after every K-th step ([ceil(T/K)][N][B]),
+ *             with K = 0 the pre-reset potential of every step ([T][N][B]).
+ *   backward: fast-sigmoid surrogate 1 / (1 + slope |x|)^2; grad_w [S] is
+ *             overwritten, grad_ext may be NULL.  Recomputes each K-step
+ *             segment from the checkpoints when K > 0. */
+typedef struct snc_b200_bptt snc_b200_bptt;
+int snc_b200_bptt_create(int32_t num_neurons, int32_t num_synapses, const int32_t* row_ptr,
+                         const int32_t* post, const int32_t* delays, snc_b200_bptt** out);
+int snc_b200_bptt_release(snc_b200_bptt* h);
+int snc_b200_bptt_forward(snc_b200_bptt* h, const float* w, const float* ext, int32_t T, int32_t B,
+                          float threshold, float decay, float slope, int32_t ckpt_every,
+                          int32_t smooth, float* spikes, uint32_t* spike_bits, float* v_saved,
+                          void* stream);
+int snc_b200_bptt_backward(snc_b200_bptt* h, const float* w, const float* ext, int32_t T, int32_t B,
+                           float threshold, float decay, float slope, int32_t ckpt_every,
+                           int32_t smooth, const float* spikes, const uint32_t* spike_bits,
+                           const float* v_saved, const float* grad_spikes, float* grad_w,
+                           float* grad_ext, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,499 @@
+// Surrogate-gradient BPTT over the sparse delayed graph: a forward and a
+// custom backward kernel behind torch.autograd.Function (snc_b200/bptt.py).
+//
+// Model (python/snc/model.py:52-72 with the per-synapse delays of
+// python/snc/shd_model.py:109-121; restated in oracle/bptt_ref.py):
+//   cur_j(t) = sum_{e: post(e)=j} w_e * s_pre(e)(t - d_e)      (0 for t-d < 0)
+//   vp_j(t)  = decay * v_j(t-1) + cur_j(t) + ext_j(t)
+//   s_j(t)   = H(vp_j(t) - thr)   [smooth variant: x / (1 + k|x|)]
+//   v_j(t)   = vp_j(t) * (1 - s_j(t))
+// Backward (reverse time), with G = dL/dvp and the fast-sigmoid surrogate
+// sg(x) = 1 / (1 + k|x|)^2:
+//   gs_i(t)  = dL/ds_i(t) + sum_{e: pre(e)=i} w_e * G_post(e)(t + d_e) - gv_i(t) * vp_i(t)
+//   G_i(t)   = gv_i(t) * (1 - s_i(t)) + gs_i(t) * sg(vp_i(t) - thr)
+//   gv_i(t-1)= decay * G_i(t);   dL/dext_i(t) = G_i(t)
+//   dL/dw_e += G_post(e)(t) * s_pre(e)(t - d_e)
+//
+// Layout: every per-neuron quantity is [.. ][N][B] with the batch innermost;
+// a warp owns a neuron, lane l holds batch elements l, l+32, ...  Binary
+// spikes are kept as a bit history [T][N][ceil(B/32)], so one in-edge costs
+// one broadcast 32-bit load per 32 samples in the forward and only the set
+// bits are visited in the weight gradient.  The incoming edges of a neuron
+// are summed in ascending CSR edge order (the order of torch's CPU
+// index_add), with separately rounded operations, so the forward spikes equal
+// the autograd model's bit for bit.  Steps are separated by a bounded grid
+// barrier inside one persistent cooperative launch.  With checkpointing
+// (every K steps) only v at segment ends is stored; the backward recomputes
+// vp for one segment at a time from those checkpoints and the stored spikes.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "device_common.cuh"
+#include "internal.h"
+
+struct snc_b200_bptt {
+  int N = 0, S = 0, D = 1, R = 2, sm_count = 0;
+  int *row_ptr = nullptr, *out_post = nullptr, *out_d = nullptr;
+  int *col_ptr = nullptr, *in_pre = nullptr, *in_d = nullptr, *in_eidx = nullptr;
+  float *v = nullptr, *gv = nullptr, *gcur = nullptr, *seg = nullptr;
+  size_t v_cap = 0, gv_cap = 0, gcur_cap = 0, seg_cap = 0;
+  unsigned* ctl = nullptr;
+  int* err = nullptr;
+};
+
+namespace sncb {
+
+struct BpArgs {
+  int N, S, R, T, B, K, smooth;
+  float thr, decay, slope;
+  const int *row_ptr, *out_post, *out_d, *col_ptr, *in_pre, *in_d, *in_eidx;
+  const float* w;
+  const float* ext;    // [T][N][B]
+  float* spikes;       // [T][N][B]
+  uint32_t* bits;      // [T][N][KB]
+  float* vsaved;       // K > 0: [T/K][N][B] v at segment ends; K == 0: [T][N][B] vp
+  float* v;            // [N][B]
+  const float* gspk;   // [T][N][B]
+  float* gw;           // [S]
+  float* gext;         // [T][N][B] or null
+  float* gv;           // [N][B]
+  float* gcur;         // [R][N][B]
+  float* seg;          // [K][N][B]
+  unsigned* ctl;
+  int* err;
+};
+
+constexpr int kBpThreads = 256;
+
+// One step of the forward for neuron j.  v holds the neuron's state before
+// the step (per lane, batch elements lane + 32k) and is updated; vp receives
+// the pre-reset potential; s the spike.
+template <int KB, bool SMOOTH>
+__device__ __forceinline__ void fwd_neuron(const BpArgs& a, int t, int j, float (&v)[KB],
+                                           float (&vp)[KB], float (&s)[KB]) {
+  const int lane = threadIdx.x & 31;
+  float acc[KB];
+#pragma unroll
+  for (int k = 0; k < KB; ++k) acc[k] = 0.f;
+  const int e0 = a.col_ptr[j], e1 = a.col_ptr[j + 1];
+  for (int eb = e0; eb < e1; eb += 32) {
+    const int n = min(32, e1 - eb);
+    int my_pre = 0, my_d = 1 << 30;
+    float my_w = 0.f;
+    if (lane < n) {
+      my_pre = a.in_pre[eb + lane];
+      my_d = a.in_d[eb + lane];
+      my_w = a.w[a.in_eidx[eb + lane]];
+    }
+    for (int q = 0; q < n; ++q) {
+      const int pre = __shfl_sync(0xffffffffu, my_pre, q);
+      const int d = __shfl_sync(0xffffffffu, my_d, q);
+      const float ww = __shfl_sync(0xffffffffu, my_w, q);
+      const int ts = t - d;
+      if (ts < 0) continue;
+      if (!SMOOTH) {
+        const uint32_t* wp = a.bits + ((size_t)ts * a.N + pre) * KB;
+#pragma unroll
+        for (int k = 0; k < KB; ++k)
+          if ((wp[k] >> lane) & 1u) acc[k] = __fadd_rn(acc[k], ww);
+      } else {
+        const float* sp = a.spikes + ((size_t)ts * a.N + pre) * a.B;
+#pragma unroll
+        for (int k = 0; k < KB; ++k) {
+          const int b = 32 * k + lane;
+          if (b < a.B) acc[k] = __fadd_rn(acc[k], __fmul_rn(ww, sp[b]));
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < KB; ++k) {
+    const int b = 32 * k + lane;
+    const float x_ext = b < a.B ? a.ext[((size_t)t * a.N + j) * a.B + b] : 0.f;
+    vp[k] = __fadd_rn(__fadd_rn(__fmul_rn(a.decay, v[k]), acc[k]), x_ext);
+    const float x = __fsub_rn(vp[k], a.thr);
+    s[k] = SMOOTH ? __fdiv_rn(x, __fadd_rn(1.f, __fmul_rn(a.slope, fabsf(x)))) : (x >= 0.f ? 1.f : 0.f);
+    v[k] = __fmul_rn(vp[k], __fsub_rn(1.f, s[k]));
+  }
+}
+
+template <int KB, bool SMOOTH>
+__global__ void __launch_bounds__(kBpThreads) k_bptt_forward(BpArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int W = (gridDim.x * blockDim.x) >> 5;
+  const unsigned nb = gridDim.x;
+  unsigned target = 0;
+  for (int j = gw; j < a.N; j += W)
+#pragma unroll
+    for (int k = 0; k < KB; ++k) {
+      const int b = 32 * k + lane;
+      if (b < a.B) a.v[(size_t)j * a.B + b] = 0.f;
+    }
+  for (int t = 0; t < a.T; ++t) {
+    for (int j = gw; j < a.N; j += W) {
+      float v[KB], vp[KB], s[KB];
+#pragma unroll
+      for (int k = 0; k < KB; ++k) {
+        const int b = 32 * k + lane;
+        v[k] = b < a.B ? a.v[(size_t)j * a.B + b] : 0.f;
+      }
+      fwd_neuron<KB, SMOOTH>(a, t, j, v, vp, s);
+      const size_t plane = ((size_t)t * a.N + j) * a.B;
+#pragma unroll
+      for (int k = 0; k < KB; ++k) {
+        const int b = 32 * k + lane;
+        const bool ok = b < a.B;
+        if (ok) {
+          a.v[(size_t)j * a.B + b] = v[k];
+          a.spikes[plane + b] = s[k];
+          if (a.K == 0) a.vsaved[plane + b] = vp[k];
+          else if ((t + 1) % a.K == 0) a.vsaved[((size_t)(t / a.K) * a.N + j) * a.B + b] = v[k];
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, ok && s[k] != 0.f);
+        if (!SMOOTH && lane == 0) a.bits[((size_t)t * a.N + j) * KB + k] = m;
+      }
+    }
+    target += nb;
+    if (!grid_sync(&a.ctl[0], target, a.err)) return;
+  }
+}
+
+// One backward step for neuron i; vp_plane points at the [N][B] plane of
+// pre-reset potentials of step t.  sm_g: this warp's [B] scratch.
+template <int KB, bool SMOOTH>
+__device__ __forceinline__ void bwd_neuron(const BpArgs& a, int t, int i, const float* vp_plane,
+                                           float* sm_g) {
+  const int lane = threadIdx.x & 31;
+  const int N = a.N, B = a.B;
+  float gs[KB];
+  const size_t plane = ((size_t)t * N + i) * B;
+#pragma unroll
+  for (int k = 0; k < KB; ++k) {
+    const int b = 32 * k + lane;
+    gs[k] = b < B ? a.gspk[plane + b] : 0.f;
+  }
+  // gradient reaching s_i(t) through every outgoing synapse (fires at t + d)
+  const int e0 = a.row_ptr[i], e1 = a.row_ptr[i + 1];
+  for (int eb = e0; eb < e1; eb += 32) {
+    const int n = min(32, e1 - eb);
+    int my_post = 0, my_d = 1 << 30;
+    float my_w = 0.f;
+    if (lane < n) {
+      my_post = a.out_post[eb + lane];
+      my_d = a.out_d[eb + lane];
+      my_w = a.w[eb + lane];
+    }
+    for (int q = 0; q < n; ++q) {
+      const int post = __shfl_sync(0xffffffffu, my_post, q);
+      const int d = __shfl_sync(0xffffffffu, my_d, q);
+      const float ww = __shfl_sync(0xffffffffu, my_w, q);
+      const int tt = t + d;
+      if (tt >= a.T) continue;
+      const float* gp = a.gcur + ((size_t)(tt % a.R) * N + post) * B;
+#pragma unroll
+      for (int k = 0; k < KB; ++k) {
+        const int b = 32 * k + lane;
+        if (b < B) gs[k] = __fadd_rn(gs[k], __fmul_rn(ww, gp[b]));
+      }
+    }
+  }
+  float* gc = a.gcur + ((size_t)(t % a.R) * N + i) * B;
+#pragma unroll
+  for (int k = 0; k < KB; ++k) {
+    const int b = 32 * k + lane;
+    if (b >= B) continue;
+    const float vp = vp_plane[(size_t)i * B + b];
+    const float x = __fsub_rn(vp, a.thr);
+    const float den = __fadd_rn(1.f, __fmul_rn(a.slope, fabsf(x)));
+    const float s = SMOOTH ? __fdiv_rn(x, den) : (x >= 0.f ? 1.f : 0.f);
+    const float sg = __fdiv_rn(1.f, __fmul_rn(den, den));
+    const float gvv = a.gv[(size_t)i * B + b];
+    const float gst = __fsub_rn(gs[k], __fmul_rn(gvv, vp));
+    const float g = __fadd_rn(__fmul_rn(gvv, __fsub_rn(1.f, s)), __fmul_rn(gst, sg));
+    gc[b] = g;
+    if (a.gext) a.gext[plane + b] = g;
+    a.gv[(size_t)i * B + b] = __fmul_rn(a.decay, g);
+    sm_g[b] = g;
+  }
+  __syncwarp();
+  // dL/dw for every incoming synapse: lane per synapse, sum of G over the
+  // samples whose pre neuron fired at t - d (only set bits are visited)
+  const int c0 = a.col_ptr[i], c1 = a.col_ptr[i + 1];
+  for (int e = c0 + lane; e < c1; e += 32) {
+    const int ts = t - a.in_d[e];
+    if (ts < 0) continue;
+    const int pre = a.in_pre[e];
+    float c = 0.f;
+    if (!SMOOTH) {
+      const uint32_t* wp = a.bits + ((size_t)ts * N + pre) * KB;
+#pragma unroll
+      for (int k = 0; k < KB; ++k) {
+        uint32_t word = wp[k];
+        while (word) {
+          const int bb = __ffs(word) - 1;
+          c = __fadd_rn(c, sm_g[32 * k + bb]);
+          word &= word - 1u;
+        }
+      }
+    } else {
+      const float* sp = a.spikes + ((size_t)ts * N + pre) * B;
+      for (int b = 0; b < B; ++b) c = __fadd_rn(c, __fmul_rn(sm_g[b], sp[b]));
+    }
+    if (c != 0.f) a.gw[a.in_eidx[e]] = __fadd_rn(a.gw[a.in_eidx[e]], c);
+  }
+  __syncwarp();
+}
+
+template <int KB, bool SMOOTH>
+__global__ void __launch_bounds__(kBpThreads) k_bptt_backward(BpArgs a) {
+  extern __shared__ float sm_all[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  float* sm_g = sm_all + (size_t)wib * (32 * KB);
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int W = (gridDim.x * blockDim.x) >> 5;
+  const unsigned nb = gridDim.x;
+  const size_t NB = (size_t)a.N * a.B;
+  unsigned target = 0;
+  for (int i = gw; i < a.N; i += W)
+#pragma unroll
+    for (int k = 0; k < KB; ++k) {
+      const int b = 32 * k + lane;
+      if (b < a.B) a.gv[(size_t)i * a.B + b] = 0.f;
+    }
+  if (a.K == 0) {
+    for (int t = a.T - 1; t >= 0; --t) {
+      for (int i = gw; i < a.N; i += W) bwd_neuron<KB, SMOOTH>(a, t, i, a.vsaved + (size_t)t * NB, sm_g);
+      target += nb;
+      if (!grid_sync(&a.ctl[0], target, a.err)) return;
+    }
+    return;
+  }
+  const int nseg = (a.T + a.K - 1) / a.K;
+  for (int sg = nseg - 1; sg >= 0; --sg) {
+    const int t0 = sg * a.K, t1 = min(a.T, t0 + a.K);
+    // recompute the segment's pre-reset potentials of this warp's neurons
+    // from the checkpoint and the stored spikes (no cross-neuron dependence)
+    for (int i = gw; i < a.N; i += W) {
+      float v[KB], vp[KB], s[KB];
+#pragma unroll
+      for (int k = 0; k < KB; ++k) {
+        const int b = 32 * k + lane;
+        v[k] = (sg > 0 && b < a.B) ? a.vsaved[(size_t)(sg - 1) * NB + (size_t)i * a.B + b] : 0.f;
+      }
+      for (int t = t0; t < t1; ++t) {
+        fwd_neuron<KB, SMOOTH>(a, t, i, v, vp, s);
+#pragma unroll
+        for (int k = 0; k < KB; ++k) {
+          const int b = 32 * k + lane;
+          if (b < a.B) a.seg[(size_t)(t - t0) * NB + (size_t)i * a.B + b] = vp[k];
+        }
+      }
+    }
+    for (int t = t1 - 1; t >= t0; --t) {
+      for (int i = gw; i < a.N; i += W)
+        bwd_neuron<KB, SMOOTH>(a, t, i, a.seg + (size_t)(t - t0) * NB, sm_g);
+      target += nb;
+      if (!grid_sync(&a.ctl[0], target, a.err)) return;
+    }
+  }
+}
+
+template <typename F>
+static int coop_launch(F kern, const BpArgs& a, int sm_count, size_t smem, cudaStream_t st) {
+  SNCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  SNCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBpThreads, smem));
+  if (per_sm < 1) {
+    set_error("bptt kernel does not fit on an SM");
+    return SNC_B200_EUNSUPPORTED;
+  }
+  const int warps_needed = a.N;
+  const int blocks = std::max(1, std::min(per_sm * sm_count, (warps_needed + 7) / 8));
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(kBpThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  SNCB_CUDA(cudaLaunchKernelEx(&cfg, kern, a));
+  return SNC_B200_OK;
+}
+
+template <int KB>
+static int dispatch(bool forward, bool smooth, const BpArgs& a, int sm, cudaStream_t st) {
+  const size_t smem = (size_t)(kBpThreads / 32) * 32 * KB * sizeof(float);
+  if (forward)
+    return smooth ? coop_launch(k_bptt_forward<KB, true>, a, sm, 0, st)
+                  : coop_launch(k_bptt_forward<KB, false>, a, sm, 0, st);
+  return smooth ? coop_launch(k_bptt_backward<KB, true>, a, sm, smem, st)
+                : coop_launch(k_bptt_backward<KB, false>, a, sm, smem, st);
+}
+
+static int launch(bool forward, bool smooth, const BpArgs& a, int sm, cudaStream_t st) {
+  const int KB = (a.B + 31) / 32;
+  if (KB <= 1) return dispatch<1>(forward, smooth, a, sm, st);
+  if (KB <= 2) return dispatch<2>(forward, smooth, a, sm, st);
+  if (KB <= 4) return dispatch<4>(forward, smooth, a, sm, st);
+  if (KB <= 8) return dispatch<8>(forward, smooth, a, sm, st);
+  set_error("bptt: batch > 256");
+  return SNC_B200_EUNSUPPORTED;
+}
+
+template <typename T>
+static int grow(T** p, size_t* cap, size_t n) {
+  if (*p && *cap >= n) return SNC_B200_OK;
+  dev_free(*p);
+  *p = nullptr;
+  *cap = 0;
+  int rc = dev_alloc(p, n);
+  if (!rc) *cap = n;
+  return rc;
+}
+
+static int check_err(snc_b200_bptt* h, cudaStream_t st) {
+  int err = 0;
+  SNCB_CUDA(cudaMemcpyAsync(&err, h->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SNCB_CUDA(cudaStreamSynchronize(st));
+  if (err) {
+    set_error("bptt: device barrier timed out");
+    return err;
+  }
+  return SNC_B200_OK;
+}
+
+}  // namespace sncb
+
+using namespace sncb;
+
+extern "C" {
+
+int snc_b200_bptt_create(int32_t N, int32_t S, const int32_t* row_ptr, const int32_t* post,
+                         const int32_t* delays, snc_b200_bptt** out) {
+  if (!out || N <= 0 || S < 0 || !row_ptr || (S > 0 && (!post || !delays)) || row_ptr[0] != 0 ||
+      row_ptr[N] != S) {
+    set_error("bptt_create: bad graph");
+    return SNC_B200_EINVAL;
+  }
+  for (int i = 0; i < N; ++i)
+    if (row_ptr[i] > row_ptr[i + 1]) { set_error("bptt_create: row_ptr not monotone"); return SNC_B200_EINVAL; }
+  int D = 1;
+  for (int e = 0; e < S; ++e) {
+    if (post[e] < 0 || post[e] >= N || delays[e] < 1) { set_error("bptt_create: bad edge"); return SNC_B200_EINVAL; }
+    D = std::max(D, delays[e]);
+  }
+  *out = nullptr;
+  auto* h = new snc_b200_bptt();
+  h->N = N;
+  h->S = S;
+  h->D = D;
+  h->R = D + 1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, dev);
+  // incoming lists in ascending CSR edge order
+  std::vector<int> col_ptr(N + 1, 0), in_pre(std::max(1, S)), in_d(std::max(1, S)), in_eidx(std::max(1, S));
+  for (int e = 0; e < S; ++e) col_ptr[post[e] + 1]++;
+  for (int j = 0; j < N; ++j) col_ptr[j + 1] += col_ptr[j];
+  std::vector<int> fill(col_ptr.begin(), col_ptr.end() - 1);
+  for (int i = 0; i < N; ++i)
+    for (int e = row_ptr[i]; e < row_ptr[i + 1]; ++e) {
+      const int q = fill[post[e]]++;
+      in_pre[q] = i;
+      in_d[q] = delays[e];
+      in_eidx[q] = e;
+    }
+  int rc = SNC_B200_OK;
+  if (!rc) rc = dev_upload(&h->row_ptr, row_ptr, (size_t)N + 1);
+  if (!rc) rc = dev_upload(&h->out_post, post, (size_t)std::max(1, S));
+  if (!rc) rc = dev_upload(&h->out_d, delays, (size_t)std::max(1, S));
+  if (!rc) rc = dev_upload(&h->col_ptr, col_ptr.data(), col_ptr.size());
+  if (!rc) rc = dev_upload(&h->in_pre, in_pre.data(), in_pre.size());
+  if (!rc) rc = dev_upload(&h->in_d, in_d.data(), in_d.size());
+  if (!rc) rc = dev_upload(&h->in_eidx, in_eidx.data(), in_eidx.size());
+  if (!rc) rc = dev_alloc(&h->ctl, 4);
+  if (!rc) rc = dev_alloc(&h->err, 1);
+  if (rc) {
+    snc_b200_bptt_release(h);
+    return rc;
+  }
+  *out = h;
+  return SNC_B200_OK;
+}
+
+int snc_b200_bptt_release(snc_b200_bptt* h) {
+  if (!h) return SNC_B200_OK;
+  for (void* p : {(void*)h->row_ptr, (void*)h->out_post, (void*)h->out_d, (void*)h->col_ptr,
+                  (void*)h->in_pre, (void*)h->in_d, (void*)h->in_eidx, (void*)h->v, (void*)h->gv,
+                  (void*)h->gcur, (void*)h->seg, (void*)h->ctl, (void*)h->err})
+    dev_free(p);
+  delete h;
+  return SNC_B200_OK;
+}
+
+int snc_b200_bptt_forward(snc_b200_bptt* h, const float* w, const float* ext, int32_t T, int32_t B,
+                          float threshold, float decay, float slope, int32_t ckpt_every,
+                          int32_t smooth, float* spikes, uint32_t* spike_bits, float* v_saved,
+                          void* stream) {
+  if (!h || !w || !ext || !spikes || !v_saved || T < 1 || B < 1 || ckpt_every < 0 ||
+      (!smooth && !spike_bits)) {
+    set_error("bptt_forward: bad argument");
+    return SNC_B200_EINVAL;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t NB = (size_t)h->N * B;
+  int rc = grow(&h->v, &h->v_cap, NB);
+  if (rc) return rc;
+  BpArgs a{};
+  a.N = h->N; a.S = h->S; a.R = h->R; a.T = T; a.B = B; a.K = ckpt_every; a.smooth = smooth;
+  a.thr = threshold; a.decay = decay; a.slope = slope;
+  a.row_ptr = h->row_ptr; a.out_post = h->out_post; a.out_d = h->out_d; a.col_ptr = h->col_ptr;
+  a.in_pre = h->in_pre; a.in_d = h->in_d; a.in_eidx = h->in_eidx;
+  a.w = w; a.ext = ext; a.spikes = spikes; a.bits = spike_bits; a.vsaved = v_saved; a.v = h->v;
+  a.ctl = h->ctl; a.err = h->err;
+  SNCB_CUDA(cudaMemsetAsync(h->ctl, 0, 16, st));
+  SNCB_CUDA(cudaMemsetAsync(h->err, 0, 4, st));
+  if ((rc = launch(true, smooth != 0, a, h->sm_count, st))) return rc;
+  return check_err(h, st);
+}
+
+int snc_b200_bptt_backward(snc_b200_bptt* h, const float* w, const float* ext, int32_t T, int32_t B,
+                           float threshold, float decay, float slope, int32_t ckpt_every,
+                           int32_t smooth, const float* spikes, const uint32_t* spike_bits,
+                           const float* v_saved, const float* grad_spikes, float* grad_w,
+                           float* grad_ext, void* stream) {
+  if (!h || !w || !ext || !spikes || !v_saved || !grad_spikes || !grad_w || T < 1 || B < 1 ||
+      ckpt_every < 0 || (!smooth && !spike_bits)) {
+    set_error("bptt_backward: bad argument");
+    return SNC_B200_EINVAL;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t NB = (size_t)h->N * B;
+  int rc;
+  if ((rc = grow(&h->v, &h->v_cap, NB))) return rc;
+  if ((rc = grow(&h->gv, &h->gv_cap, NB))) return rc;
+  if ((rc = grow(&h->gcur, &h->gcur_cap, (size_t)h->R * NB))) return rc;
+  if (ckpt_every > 0 && (rc = grow(&h->seg, &h->seg_cap, (size_t)ckpt_every * NB))) return rc;
+  BpArgs a{};
+  a.N = h->N; a.S = h->S; a.R = h->R; a.T = T; a.B = B; a.K = ckpt_every; a.smooth = smooth;
+  a.thr = threshold; a.decay = decay; a.slope = slope;
+  a.row_ptr = h->row_ptr; a.out_post = h->out_post; a.out_d = h->out_d; a.col_ptr = h->col_ptr;
+  a.in_pre = h->in_pre; a.in_d = h->in_d; a.in_eidx = h->in_eidx;
+  a.w = w; a.ext = ext; a.spikes = const_cast<float*>(spikes);
+  a.bits = const_cast<uint32_t*>(spike_bits); a.vsaved = const_cast<float*>(v_saved); a.v = h->v;
+  a.gspk = grad_spikes; a.gw = grad_w; a.gext = grad_ext; a.gv = h->gv; a.gcur = h->gcur; a.seg = h->seg;
+  a.ctl = h->ctl; a.err = h->err;
+  SNCB_CUDA(cudaMemsetAsync(h->ctl, 0, 16, st));
+  SNCB_CUDA(cudaMemsetAsync(h->err, 0, 4, st));
+  SNCB_CUDA(cudaMemsetAsync(grad_w, 0, (size_t)std::max(1, h->S) * sizeof(float), st));
+  if ((rc = launch(false, smooth != 0, a, h->sm_count, st))) return rc;
+  return check_err(h, st);
+}
+
+}  // extern "C"

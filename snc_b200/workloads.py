@@ -264,3 +264,67 @@ def random_events(seed, g: SNNGraph, num_samples, steps, rate=0.2, amp_jitter=Tr
         evs.append(np.concatenate([ev, extra]))
     ev = np.concatenate(evs)
     return ev[rng.permutation(ev.shape[0])], np.array(steps, np.int32)
+
+
+# ---------------------------------------------------------------------------
+# BPTT workloads
+# ---------------------------------------------------------------------------
+
+def layered_local_edges(layers, fanout, seed=1, max_delay=4):
+    """Feed-forward layers with 1-D local receptive fields: every pre in layer
+    l projects to a contiguous window of `fanout` neurons of layer l+1 centred
+    on its relative position (the make_static_snc pattern,
+    src/graph/snn_graph.cpp:185-236).  Delays U{1..max_delay}."""
+    rng = np.random.default_rng(seed)
+    pres, posts = [], []
+    base = 0
+    for l in range(len(layers) - 1):
+        a_n, b_n = layers[l], layers[l + 1]
+        k = min(fanout, b_n)
+        pos = np.arange(a_n) / max(1, a_n - 1)
+        centre = np.clip(np.rint(pos * (b_n - 1)).astype(np.int64), 0, b_n - 1)
+        lo = np.clip(centre - k // 2, 0, b_n - k)
+        pres.append(np.repeat(np.arange(a_n) + base, k))
+        posts.append((lo[:, None] + np.arange(k)[None, :]).ravel() + base + a_n)
+        base += a_n
+    pre, post = np.concatenate(pres), np.concatenate(posts)
+    return pre, post, rng.integers(1, max_delay + 1, pre.shape[0])
+
+
+def bptt_mnist_like(seed=1, T=100, B=128, rate=0.2):
+    """784 Poisson inputs -> 512 -> 512 LIF (local sparse, ~6x fewer synapses
+    than dense, delays 1-4) -> 10 leaky readout; input spikes [T, B, 784],
+    random labels."""
+    layers = [784, 512, 512]
+    dense = 784 * 512 + 512 * 512
+    fanout = int(round(dense / 6 / (784 + 512)))
+    pre, post, d = layered_local_edges(layers, fanout, seed=seed, max_delay=4)
+    rng = np.random.default_rng([seed, 2])
+    x = rng.random((B, 784), dtype=np.float32) * np.float32(rate)
+    spikes = (rng.random((T, B, 784), dtype=np.float32) < x[None]).astype(np.float32)
+    labels = rng.integers(0, 10, B)
+    readout_ids = np.arange(784 + 512, 784 + 1024)
+    return {"N": 1808, "pre": pre, "post": post, "delays": d, "n_in": 784,
+            "readout_ids": readout_ids, "spikes": spikes, "labels": labels}
+
+
+def zipf_tokens(rng, vocab, n, s=1.1):
+    p = 1.0 / np.arange(1, vocab + 1) ** s
+    return rng.choice(vocab, size=n, p=p / p.sum())
+
+
+def char_lm(seed=1, vocab=96, hidden=4096, fan_in=64, sigma=64.0, max_delay=8, B=64, T=256):
+    """Spiking char-LM: recurrent hidden neurons with fan-in 64 drawn by a
+    Gaussian over ring distance (locality-biased), delays U{1..8}; token ids
+    from a seeded Zipf(1.1) sequence (no text corpus)."""
+    rng = np.random.default_rng(seed)
+    post = np.repeat(np.arange(hidden), fan_in)
+    off = np.rint(rng.normal(0, sigma, post.shape[0])).astype(np.int64)
+    off[off == 0] = 1
+    pre = (post + off) % hidden
+    order = np.argsort(pre, kind="stable")
+    pre, post = pre[order], post[order]
+    d = rng.integers(1, max_delay + 1, pre.shape[0])
+    tokens = zipf_tokens(rng, vocab, B * (T + 1)).reshape(B, T + 1)
+    return {"H": hidden, "vocab": vocab, "pre": pre, "post": post, "delays": d,
+            "x": tokens[:, :T], "y": tokens[:, 1:]}

@@ -1,0 +1,166 @@
+"""The custom BPTT kernels against the autograd restatement of the bridge
+(oracle/bptt_ref.py, pinned to the reference's SNN / SHDNet in
+tests/test_bptt_ref.py).
+
+Forward spikes must be bit-identical (the incoming edges are summed in the
+order of torch's CPU index_add with the same roundings); gradients agree
+within 1e-4 relative to their largest magnitude; checkpointing with
+recompute changes nothing; the smoothed variant matches finite differences.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import bptt_ref as BR
+from snc_b200 import bptt as BP
+from snc_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+
+
+def graph(seed, n_in=24, n_hid=70, n_out=6, max_delay=4):
+    g = W.random_graph(seed, n_in=n_in, n_hid=n_hid, n_out=n_out, max_delay=max_delay, w_scale=0.8)
+    rng = np.random.default_rng(seed)
+    w = (rng.normal(0, 0.6, g.num_synapses) * np.where(rng.random(g.num_synapses) < 0.3, -1, 1)).astype(np.float32)
+    return g, w
+
+
+def ref_run(g, w, ext, thr, decay, k, proj, smooth=False, dtype=torch.float32):
+    wt = torch.as_tensor(w, dtype=dtype).clone().requires_grad_(True)
+    et = ext.to(dtype).clone().requires_grad_(True)
+    s = BR.core_forward(wt, et, torch.as_tensor(g.pre_ids()).long(), torch.as_tensor(g.post_ids).long(),
+                        torch.as_tensor(g.delays).long(), thr, decay, k, smooth=smooth)
+    (s * proj.to(dtype)).sum().backward()
+    return s.detach(), wt.grad, et.grad
+
+
+def gpu_run(g, w, ext, thr, decay, k, proj, ckpt, smooth=False):
+    core = BP.SpikingCore(g.num_neurons, g.pre_ids(), g.post_ids, g.delays, device=DEV)
+    wt = torch.as_tensor(w, device=DEV).clone().requires_grad_(True)
+    et = ext.to(DEV).clone().requires_grad_(True)
+    s = BP.spiking_core(wt, et, core, thr, decay, k, ckpt, smooth)
+    (s * proj.to(DEV)).sum().backward()
+    return s.detach().cpu(), wt.grad.cpu(), et.grad.cpu()
+
+
+def rel_close(a, b, tol=1e-4):
+    scale = max(float(b.abs().max()), 1e-12)
+    assert float((a - b).abs().max()) <= tol * scale, (float((a - b).abs().max()), scale)
+
+
+@pytest.mark.parametrize("B", [5, 32, 40, 128])
+@pytest.mark.parametrize("ckpt", [0, 3, 10])
+def test_forward_exact_and_gradients(B, ckpt):
+    g, w = graph(1)
+    T = 23
+    gen = torch.Generator().manual_seed(B)
+    ext = (torch.rand(T, B, g.num_neurons, generator=gen) < 0.25).float() * 1.1
+    ext[:, :, 24:] = 0.0
+    proj = torch.randn(T, B, g.num_neurons, generator=gen)
+    s_ref, gw_ref, ge_ref = ref_run(g, w, ext, 1.0, 0.9, 25.0, proj)
+    s, gw, ge = gpu_run(g, w, ext, 1.0, 0.9, 25.0, proj, ckpt)
+    assert s_ref.sum() > 0
+    assert torch.equal(s, s_ref)
+    rel_close(gw, gw_ref)
+    rel_close(ge, ge_ref)
+
+
+def test_checkpointing_is_exact():
+    g, w = graph(2, max_delay=7)
+    T, B = 31, 16
+    gen = torch.Generator().manual_seed(0)
+    ext = torch.rand(T, B, g.num_neurons, generator=gen) * 0.6
+    proj = torch.randn(T, B, g.num_neurons, generator=gen)
+    outs = [gpu_run(g, w, ext, 1.0, 0.95, 25.0, proj, k) for k in (0, 1, 4, 10, 64)]
+    for o in outs[1:]:
+        assert torch.equal(o[0], outs[0][0])
+        assert torch.equal(o[1], outs[0][1])
+        assert torch.equal(o[2], outs[0][2])
+
+
+def test_smooth_variant_against_fp64_and_finite_differences():
+    g, w = graph(3, n_hid=40, max_delay=3)
+    w = (w * 0.5).astype(np.float32)
+    T, B = 12, 8
+    gen = torch.Generator().manual_seed(1)
+    ext = torch.rand(T, B, g.num_neurons, generator=gen)
+    proj = torch.randn(T, B, g.num_neurons, generator=gen)
+    _, gw64, ge64 = ref_run(g, w, ext, 0.5, 0.9, 5.0, proj, smooth=True, dtype=torch.float64)
+    _, gw, ge = gpu_run(g, w, ext, 0.5, 0.9, 5.0, proj, 4, smooth=True)
+    rel_close(gw.double(), gw64, 1e-4)
+    rel_close(ge.double(), ge64, 1e-4)
+    core = BP.SpikingCore(g.num_neurons, g.pre_ids(), g.post_ids, g.delays, device=DEV)
+    e_d, p_d = ext.to(DEV), proj.to(DEV)
+
+    def loss(wv):
+        with torch.no_grad():
+            return float((BP.spiking_core(torch.as_tensor(wv, device=DEV), e_d, core, 0.5, 0.9, 5.0, 0,
+                                          True) * p_d).double().sum())
+
+    eps = 2e-3
+    for i in np.random.default_rng(0).choice(g.num_synapses, 8, replace=False):
+        wp, wm = w.copy(), w.copy()
+        wp[i] += eps
+        wm[i] -= eps
+        fd = (loss(wp) - loss(wm)) / (2 * eps)
+        assert abs(fd - float(gw[i])) <= 2e-2 * max(1.0, abs(fd)), (i, fd, float(gw[i]))
+
+
+def test_snn_dropin_matches_restatement():
+    """snc_b200.bptt.SNN with the bridge constructor, direct encoding."""
+    g, w = graph(4)
+    d = {"N": g.num_neurons, "S": g.num_synapses, "n_in": g.num_input_channels,
+         "n_out": g.num_output_channels, "pre": g.pre_ids(), "post": g.post_ids, "delays": g.delays,
+         "role": g.role.astype(np.int32), "channel": g.channel}
+    net = BP.SNN(d, num_steps=15, thr=1.0, decay=0.9, encoder="direct", surrogate_scale=25.0).to(DEV)
+    with torch.no_grad():
+        net.w.copy_(torch.as_tensor(w))
+    x = torch.rand(9, d["n_in"], generator=torch.Generator().manual_seed(5))
+    logits = net(x.to(DEV))
+    logits.square().sum().backward()
+    ext = torch.zeros(15, 9, d["N"])
+    ext[:, :, :d["n_in"]] = x
+    wt = torch.as_tensor(w).clone().requires_grad_(True)
+    s = BR.core_forward(wt, ext, torch.as_tensor(d["pre"]).long(), torch.as_tensor(d["post"]).long(),
+                        torch.as_tensor(d["delays"]).long(), 1.0, 0.9, 25.0)
+    out_ids = torch.as_tensor(np.nonzero(d["role"] == 2)[0]).long()
+    ref = torch.zeros(9, d["n_out"]).index_add(1, torch.as_tensor(d["channel"])[out_ids].long(),
+                                               s.sum(0)[:, out_ids])
+    assert torch.equal(logits.detach().cpu(), ref.detach())
+    ref.square().sum().backward()
+    rel_close(net.w.grad.cpu(), wt.grad)
+
+
+def test_spiking_lm_gradients():
+    H, V, T, B = 96, 12, 20, 8
+    rng = np.random.default_rng(6)
+    pre = np.repeat(np.arange(H), 8)
+    post = (pre + rng.integers(-6, 7, pre.shape[0])) % H
+    dl = rng.integers(1, 9, pre.shape[0])
+    torch.manual_seed(0)
+    lm = BP.SpikingLM(V, H, pre, post, dl, w_scale=2.0).to(DEV)
+    with torch.no_grad():
+        lm.embed.weight.mul_(1.5)
+    x = torch.as_tensor(rng.integers(0, V, (B, T)))
+    logits = lm(x.to(DEV))
+    loss = torch.nn.functional.cross_entropy(logits.reshape(-1, V), x.reshape(-1).to(DEV))
+    loss.backward()
+    # autograd restatement with the same parameters
+    emb = lm.embed.weight.detach().cpu().clone().requires_grad_(True)
+    wr = lm.w_rec.detach().cpu().clone().requires_grad_(True)
+    ext = emb[x].transpose(0, 1)
+    s = BR.core_forward(wr, ext, torch.as_tensor(pre).long(), torch.as_tensor(post).long(),
+                        torch.as_tensor(dl).long(), 1.0, 0.95, 25.0)
+    r = torch.zeros(B, H)
+    rs = []
+    for t in range(T):
+        r = 0.9 * r + s[t]
+        rs.append(r)
+    lg = torch.nn.functional.linear(torch.stack(rs, 1), lm.readout.weight.detach().cpu(),
+                                    lm.readout.bias.detach().cpu())
+    l2 = torch.nn.functional.cross_entropy(lg.reshape(-1, V), x.reshape(-1))
+    l2.backward()
+    assert s.sum() > 0
+    rel_close(lm.w_rec.grad.cpu(), wr.grad, 1e-4)
+    rel_close(lm.embed.weight.grad.cpu(), emb.grad, 1e-4)
