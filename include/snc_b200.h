@@ -226,6 +226,17 @@ int snc_b200_eprop_get_weights(snc_b200_eprop* s, float* w);       /* [S] */
 int snc_b200_eprop_batch(snc_b200_eprop* s, const snc_input_event* events, size_t n_events,
                          int32_t num_samples, const int32_t* steps, const int32_t* labels,
                          int train, float* counts, snc_run_stats* stats);
+/* Data-parallel e-prop.  snc_b200_eprop_gradient runs a training minibatch
+ * but, instead of updating the weights, writes grad[s] = sum_b L[b,post(s)] *
+ * E[b,s] / T_b over this call's samples into `grad` (DEVICE pointer, [S]
+ * fp32).  snc_b200_eprop_apply then sets w = clamp(w - lr * grad /
+ * total_batch, +-w_max).  Summing the gradients of disjoint sample shards
+ * (one all-reduce) and applying once equals one minibatch over their union up
+ * to the order of the float sum. */
+int snc_b200_eprop_gradient(snc_b200_eprop* s, const snc_input_event* events, size_t n_events,
+                            int32_t num_samples, const int32_t* steps, const int32_t* labels,
+                            float* grad, float* counts, snc_run_stats* stats);
+int snc_b200_eprop_apply(snc_b200_eprop* s, const float* grad, int32_t total_batch);
 /* Eligibility [B][S] of the last training minibatch. */
 int snc_b200_eprop_get_eligibility(snc_b200_eprop* s, float* elig);
 /* cudatrain::reset_stats / collect_stats: per-synapse deliveries [S] and

@@ -109,10 +109,12 @@ def forward_batched(g: SNNGraph, events, steps, lif):
 
 
 def eprop_batch(g: SNNGraph, w, events, steps, lif, *, trace_decay, gamma, lr, w_max,
-                train_hidden, bmat, labels, train=True, want_elig=False, fires=None):
+                train_hidden, bmat, labels, train=True, want_elig=False, fires=None,
+                want_grad=False):
     """Minibatch e-prop restatement (cuda_trainer.cu rule, host events).
     Returns dict(w (updated copy), counts [B, oc], elig [B, S] or None,
-    spikes, events)."""
+    grad [S] or None (want_grad: the shard gradient, w unchanged), spikes,
+    events)."""
     events = np.ascontiguousarray(events, dtype=EVENT_DTYPE)
     steps = np.ascontiguousarray(steps, dtype=np.int32)
     B = steps.shape[0]
@@ -123,16 +125,18 @@ def eprop_batch(g: SNNGraph, w, events, steps, lif, *, trace_decay, gamma, lr, w
     elig = np.zeros((B, g.num_synapses), np.float32) if want_elig else None
     bmat = np.ascontiguousarray(bmat, dtype=np.float32)
     labels = np.ascontiguousarray(labels, dtype=np.int32)
+    grad = np.zeros(g.num_synapses, np.float32) if want_grad else None
     sp, ev = C.c_int64(), C.c_int64()
     rc = lib().orc_eprop_batch(C.byref(gs), _ptr(w), _ptr(events), C.c_size_t(events.shape[0]),
                                B, _ptr(steps), C.byref(lf), C.c_float(trace_decay),
                                C.c_float(gamma), C.c_float(lr), C.c_float(w_max),
                                int(bool(train_hidden)), _ptr(bmat), _ptr(labels),
                                int(bool(train)), _ptr(counts), _ptr(elig), C.byref(sp),
-                               C.byref(ev), _ptr(fires))
+                               C.byref(ev), _ptr(fires), _ptr(grad))
     if rc:
         raise RuntimeError(f"orc_eprop_batch failed: {rc}")
-    return {"w": w, "counts": counts, "elig": elig, "spikes": sp.value, "events": ev.value}
+    return {"w": w, "counts": counts, "elig": elig, "grad": grad, "spikes": sp.value,
+            "events": ev.value}
 
 
 # ---------------------------------------------------------------------------

@@ -280,13 +280,16 @@ int orc_forward_batched(const orc_graph* g, const orc_event* ev, size_t n_ev,
  *  counts     [B][noc] output spike counts (out)
  *  elig       [B][S]   eligibility after the window (out, may be NULL)
  *  fires      [N]      per-neuron firing counts, accumulated (may be NULL)
+ *  grad_out   [S]      when not NULL (and train != 0): sum_b L*E / T_b is
+ *                     written here and w is left unchanged (the gradient of
+ *                     one data-parallel shard)
  */
 int orc_eprop_batch(const orc_graph* g, float* w, const orc_event* ev, size_t n_ev,
                     int B, const int32_t* steps, const orc_lif* lif, float trace_decay,
                     float gamma, float lr, float w_max, int train_hidden,
                     const float* bmat, const int32_t* labels, int train,
                     float* counts, float* elig, int64_t* spikes_out,
-                    int64_t* events_out, int64_t* fires) {
+                    int64_t* events_out, int64_t* fires, float* grad_out) {
   const int n = g->num_neurons, S = g->num_synapses;
   int nic, noc;
   io_counts(g, &nic, &noc);
@@ -399,7 +402,13 @@ int orc_eprop_batch(const orc_graph* g, float* w, const orc_event* ev, size_t n_
     for (int b = 1; b < B; ++b) if (steps[b] != steps[0]) uniform = 0;
     for (int s = 0; s < S; ++s) {
       float acc = 0.0f;
-      if (uniform) {
+      if (grad_out) {
+        /* data-parallel form: the shard's gradient, weights untouched */
+        for (int b = 0; b < B; ++b)
+          acc += L[(size_t)b * n + g->post_ids[s]] * E[(size_t)b * S + s] /
+                 (float)(steps[b] > 1 ? steps[b] : 1);
+        grad_out[s] = acc;
+      } else if (uniform) {
         for (int b = 0; b < B; ++b) acc += L[(size_t)b * n + g->post_ids[s]] * E[(size_t)b * S + s];
         const float lr_over_T = lr / (float)(steps[0] > 1 ? steps[0] : 1);
         float nw = w[s] - lr_over_T * acc / (float)B;

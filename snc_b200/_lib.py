@@ -73,6 +73,8 @@ SIGNATURES = {
     "snc_b200_eprop_get_weights": (C.c_int, [P, P]),
     "snc_b200_eprop_batch": (C.c_int, [P, P, C.c_size_t, I32, P, P, C.c_int, P, P]),
     "snc_b200_eprop_get_eligibility": (C.c_int, [P, P]),
+    "snc_b200_eprop_gradient": (C.c_int, [P, P, C.c_size_t, I32, P, P, P, P, P]),
+    "snc_b200_eprop_apply": (C.c_int, [P, P, I32]),
     "snc_b200_eprop_reset_stats": (C.c_int, [P]),
     "snc_b200_eprop_collect_stats": (C.c_int, [P, P, P]),
     "snc_b200_bptt_create": (C.c_int, [I32, I32, P, P, P, P]),

@@ -160,9 +160,33 @@ static int create_session(snc_b200_eprop* s, const Graph* g, const snc_lif* lif,
   return SNC_B200_OK;
 }
 
+// grad[s] = sum_b L[b, post(s)] * E[b, s] / T_b (data-parallel e-prop).
+__global__ void k_gradient(int S, int N, int B, const int* post, const int* steps, const float* L,
+                           const float* E, float* grad) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S) return;
+  const int p = post[s];
+  float acc = 0.f;
+  for (int b = 0; b < B; ++b)
+    acc = __fadd_rn(acc, __fdiv_rn(__fmul_rn(L[(size_t)b * N + p], E[(size_t)b * S + s]),
+                                   (float)max(1, steps[b])));
+  grad[s] = acc;
+}
+
+__global__ void k_apply_grad(int S, float lr, float w_max, int total_batch, const float* grad,
+                             uint2* edges) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S) return;
+  const float w = __uint_as_float(edges[s].y);
+  float nw = __fsub_rn(w, __fdiv_rn(__fmul_rn(lr, grad[s]), (float)total_batch));
+  nw = fminf(fmaxf(nw, -w_max), w_max);
+  edges[s].y = __float_as_uint(nw);
+}
+
+// train: 0 forward only, 1 update the weights, 2 write the gradient to grad.
 static int run_batch(snc_b200_eprop* s, const snc_input_event* ev, size_t n_ev, int B,
                      const int32_t* steps, const int32_t* labels, int train, float* counts_out,
-                     snc_run_stats* stats) {
+                     snc_run_stats* stats, float* grad = nullptr) {
   const Graph* g = s->g;
   if (B < 1 || B > s->max_batch || !steps || (train && !labels)) {
     set_error("e-prop batch: bad sample count, steps or labels");
@@ -214,8 +238,11 @@ static int run_batch(snc_b200_eprop* s, const snc_input_event* ev, size_t n_ev, 
     k_softmax_delta<<<grid_of(B), 256, 0, st>>>(B, oc, s->counts, s->labels, s->delta);
     k_learning_signal<<<grid_of((long long)B * N), 256, 0, st>>>(
         B, N, oc, s->cfg.train_hidden, g->role, g->channel, s->internal_row, s->bmat, s->delta, s->L);
-    k_apply<<<grid_of(S), 256, 0, st>>>(S, N, B, uniform ? 1 : 0, s->cfg.lr, lr_over_T,
-                                        s->cfg.w_max, g->post, s->steps, s->L, s->elig, s->edges);
+    if (train == 2)
+      k_gradient<<<grid_of(S), 256, 0, st>>>(S, N, B, g->post, s->steps, s->L, s->elig, grad);
+    else
+      k_apply<<<grid_of(S), 256, 0, st>>>(S, N, B, uniform ? 1 : 0, s->cfg.lr, lr_over_T,
+                                          s->cfg.w_max, g->post, s->steps, s->L, s->elig, s->edges);
     chk(cudaGetLastError(), "e-prop update kernels");
   }
   chk(cudaEventRecord(s->ev1, st), "event");
@@ -311,6 +338,22 @@ int snc_b200_eprop_batch(snc_b200_eprop* s, const snc_input_event* events, size_
                          int train, float* counts, snc_run_stats* stats) {
   if (!s) { set_error("null session"); return SNC_B200_EINVAL; }
   return run_batch(s, events, n_events, num_samples, steps, labels, train, counts, stats);
+}
+
+int snc_b200_eprop_gradient(snc_b200_eprop* s, const snc_input_event* events, size_t n_events,
+                            int32_t num_samples, const int32_t* steps, const int32_t* labels,
+                            float* grad, float* counts, snc_run_stats* stats) {
+  if (!s || !grad) { set_error("null argument"); return SNC_B200_EINVAL; }
+  return run_batch(s, events, n_events, num_samples, steps, labels, 2, counts, stats, grad);
+}
+
+int snc_b200_eprop_apply(snc_b200_eprop* s, const float* grad, int32_t total_batch) {
+  if (!s || !grad || total_batch < 1) { set_error("bad argument"); return SNC_B200_EINVAL; }
+  k_apply_grad<<<grid_of(s->g->S), 256>>>(s->g->S, s->cfg.lr, s->cfg.w_max, total_batch, grad,
+                                          s->edges);
+  SNCB_CUDA(cudaGetLastError());
+  SNCB_CUDA(cudaDeviceSynchronize());
+  return SNC_B200_OK;
 }
 
 int snc_b200_eprop_get_eligibility(snc_b200_eprop* s, float* elig) {

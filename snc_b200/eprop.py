@@ -107,6 +107,26 @@ class CudaTrainSession:
         return {"counts": counts[:, :self.g.num_output_channels], "spikes": st.spikes,
                 "events": st.synaptic_events, "ms": st.ms}
 
+    def gradient(self, events, steps, labels, grad) -> dict:
+        """Training minibatch without the update: grad (a float32 CUDA tensor
+        [S]) receives sum_b L * E / T_b over these samples."""
+        ev = _events(events)
+        steps = np.ascontiguousarray(steps, dtype=np.int32)
+        lab = np.ascontiguousarray(labels, dtype=np.int32)
+        B = steps.shape[0]
+        counts = np.zeros((B, max(1, self.g.num_output_channels)), np.float32)
+        st = _lib.RunStats()
+        check(lib().snc_b200_eprop_gradient(self.h, ptr(ev), ev.shape[0], B, ptr(steps), ptr(lab),
+                                            C.c_void_p(grad.data_ptr()), ptr(counts), C.byref(st)),
+              "eprop_gradient")
+        return {"counts": counts[:, :self.g.num_output_channels], "spikes": st.spikes,
+                "events": st.synaptic_events, "ms": st.ms}
+
+    def apply(self, grad, total_batch: int) -> None:
+        """w = clamp(w - lr * grad / total_batch) with grad a CUDA tensor [S]."""
+        check(lib().snc_b200_eprop_apply(self.h, C.c_void_p(grad.data_ptr()), int(total_batch)),
+              "eprop_apply")
+
     def eligibility(self, B) -> np.ndarray:
         e = np.zeros((B, self.g.num_synapses), np.float32)
         check(lib().snc_b200_eprop_get_eligibility(self.h, ptr(e)), "eprop_get_eligibility")

@@ -103,3 +103,29 @@ def test_train_epoch_runs():
     st = s.train_epoch(X, y, X[:8], y[:8], epoch=0)
     assert st["spikes"] > 0 and 0.0 <= st["test_acc"] <= 1.0
     E.destroy(s)
+
+
+def test_gradient_shards_and_apply():
+    """snc_b200_eprop_gradient over two sample shards, summed, then
+    snc_b200_eprop_apply == one minibatch over all samples (data-parallel
+    e-prop on one GPU, shards run one after the other)."""
+    import torch
+    from snc_b200 import parallel as PAR
+    g, ev, st, w0, fb, labels = make_case(6, 5, [30, 18, 30, 25, 9])
+    lif = R.LIFParams(refractory=1)
+    cfg = E.TrainConfig(lif=lif, lr=0.7, w_max=4.0, trace_decay=0.95)
+    s = E.CudaTrainSession(g, cfg, batch=8, weights=w0, feedback=fb)
+    total = torch.zeros(g.num_synapses, device="cuda")
+    for r in range(2):
+        e, t, l = PAR.shard_samples(ev, st, labels, r, 2)
+        part = torch.zeros(g.num_synapses, device="cuda")
+        s.gradient(e, t, l, part)
+        total += part
+    s.apply(total, 5)
+    ref = O.eprop_batch(g, w0, ev, st, lif, trace_decay=0.95, gamma=0.3, lr=0.7, w_max=4.0,
+                        train_hidden=True, bmat=fb, labels=labels)
+    np.testing.assert_allclose(s.get_weights(), ref["w"], rtol=1e-5, atol=1e-6)
+    # the DataParallelEprop wrapper at world size 1 is the same update
+    s2 = E.CudaTrainSession(g, cfg, batch=8, weights=w0, feedback=fb)
+    PAR.DataParallelEprop(s2, g.num_synapses).step(ev, st, labels)
+    np.testing.assert_allclose(s2.get_weights(), ref["w"], rtol=1e-5, atol=1e-6)

@@ -1,0 +1,93 @@
+"""Sample-sharded data-parallel e-prop on CPU ranks (gloo, world size 2).
+
+The GPU session is replaced by a stand-in that computes each shard's
+gradient with the CPU restatement and applies the update with the same
+operation order as snc_b200_eprop_apply; the test checks the sharding, the
+all-reduce and the update rule: every rank ends with identical weights, equal
+(up to float summation order) to one minibatch over all samples."""
+import os
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from oracle import oracle as O
+from snc_b200 import parallel as PAR
+from snc_b200 import runtime as R
+from snc_b200 import workloads as W
+from snc_b200.graph import INTERNAL
+
+LR, WMAX, GAMMA, TD = 0.7, 4.0, 0.3, 0.95
+
+
+def case():
+    g = W.random_graph(11, n_hid=50, max_delay=5)
+    ev, st = W.random_events(12, g, 5, [30, 18, 30, 25, 9])
+    rng = np.random.default_rng(3)
+    w0 = rng.normal(0, 0.5, g.num_synapses).astype(np.float32)
+    fb = rng.normal(0, 1.0, (int((g.role == INTERNAL).sum()), g.num_output_channels)).astype(np.float32)
+    labels = rng.integers(0, g.num_output_channels, 5).astype(np.int32)
+    return g, ev, st, w0, fb, labels
+
+
+class OracleSession:
+    def __init__(self, g, w, fb):
+        self.g, self.w, self.fb = g, w.copy(), fb
+        self.lif = R.LIFParams(refractory=1)
+
+    def gradient(self, ev, st, lab, grad):
+        r = O.eprop_batch(self.g, self.w, ev, st, self.lif, trace_decay=TD, gamma=GAMMA, lr=LR,
+                          w_max=WMAX, train_hidden=True, bmat=self.fb, labels=lab, want_grad=True)
+        grad.copy_(torch.from_numpy(r["grad"]))
+        return r
+
+    def apply(self, grad, total_batch):
+        gv = grad.numpy().astype(np.float32)
+        nw = self.w - (np.float32(LR) * gv) / np.float32(total_batch)
+        self.w = np.clip(nw, -WMAX, WMAX).astype(np.float32)
+
+
+def _worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        g, ev, st, w0, fb, labels = case()
+        s = OracleSession(g, w0, fb)
+        PAR.DataParallelEprop(s, g.num_synapses, device="cpu").step(ev, st, labels)
+        np.save(os.path.join(out, f"w{rank}.npy"), s.w)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_shard_bounds_cover_all_samples():
+    for n in (0, 1, 5, 7, 64):
+        for world in (1, 2, 3, 8):
+            spans = [PAR.shard_bounds(n, r, world) for r in range(world)]
+            assert spans[0][0] == 0 and spans[-1][1] == n
+            assert all(a[1] == b[0] for a, b in zip(spans, spans[1:]))
+            assert max(h - l for l, h in spans) - min(h - l for l, h in spans) <= 1
+
+
+def test_shard_samples_renumbers():
+    g, ev, st, w0, fb, labels = case()
+    ev1, st1, lab1 = PAR.shard_samples(ev, st, labels, 1, 2)
+    assert list(st1) == [25, 9] and list(lab1) == list(labels[3:5])
+    assert set(np.unique(ev1["sample_id"])) <= {0, 1}
+    assert len(ev1) == int(((ev["sample_id"] >= 3) & (ev["sample_id"] < 5)).sum())
+
+
+def test_data_parallel_eprop_gloo_world2(tmp_path):
+    port = 29500 + (os.getpid() % 1000)
+    mp.start_processes(_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    w_r0 = np.load(tmp_path / "w0.npy")
+    w_r1 = np.load(tmp_path / "w1.npy")
+    np.testing.assert_array_equal(w_r0, w_r1)
+    g, ev, st, w0, fb, labels = case()
+    single = O.eprop_batch(g, w0, ev, st, R.LIFParams(refractory=1), trace_decay=TD, gamma=GAMMA,
+                           lr=LR, w_max=WMAX, train_hidden=True, bmat=fb, labels=labels)
+    assert np.abs(single["w"] - w0).max() > 0
+    np.testing.assert_allclose(w_r0, single["w"], rtol=1e-5, atol=1e-6)
