@@ -273,6 +273,24 @@ int snc_b200_bptt_backward(snc_b200_bptt* h, const float* w, const float* ext, i
                            int32_t smooth, const float* spikes, const uint32_t* spike_bits,
                            const float* v_saved, const float* grad_spikes, float* grad_w,
                            float* grad_ext, void* stream);
+/* The BPTT forward for callers that must not allocate device memory when
+ * they call it (no counterpart in the reference, which allocates inside every
+ * GPU call): a stream being captured under a mode that forbids allocation, a
+ * framework whose allocator owns all device memory, a real-time loop.  Same
+ * arguments and results as snc_b200_bptt_forward; the caller still provides
+ * every input and output buffer, and the call makes no cudaMalloc / cudaFree.
+ * Its scratch -- the membrane state of num_neurons x B samples and the
+ * barrier / error words -- is one static 4 MiB array per device that every
+ * device loading the library keeps until exit, so num_neurons * B must not
+ * exceed 1,048,512 (SNC_B200_EUNSUPPORTED otherwise).  All calls share that
+ * array: calls whose work overlaps on the GPU (different streams, threads or
+ * handles without ordering) race and must not be issued.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture. */
+int snc_b200_bptt_forward_static(snc_b200_bptt* h, const float* w, const float* ext, int32_t T,
+                                 int32_t B, float threshold, float decay, float slope,
+                                 int32_t ckpt_every, int32_t smooth, float* spikes,
+                                 uint32_t* spike_bits, float* v_saved, void* stream);
 
 #ifdef __cplusplus
 }

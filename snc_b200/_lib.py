@@ -83,6 +83,8 @@ SIGNATURES = {
                                         I32, P, P, P, P]),
     "snc_b200_bptt_backward": (C.c_int, [P, P, P, I32, I32, C.c_float, C.c_float, C.c_float, I32,
                                          I32, P, P, P, P, P, P, P]),
+    "snc_b200_bptt_forward_static": (C.c_int, [P, P, P, I32, I32, C.c_float, C.c_float, C.c_float,
+                                               I32, I32, P, P, P, P]),
 }
 
 _LIB = None

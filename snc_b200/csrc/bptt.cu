@@ -497,3 +497,100 @@ int snc_b200_bptt_backward(snc_b200_bptt* h, const float* w, const float* ext, i
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Forward without device allocation.
+//
+// Some callers cannot allocate device memory at the moment they run the
+// forward: code executing while a stream is being captured into a CUDA graph
+// under a capture mode that forbids allocation, frameworks whose caching
+// allocator owns all device memory and treats any allocation outside it as an
+// error, and real-time loops that must not pay cudaMalloc's latency or risk
+// its failure.  snc_b200_bptt_forward may allocate on its first use at a
+// given size (the per-neuron state buffer of the handle grows on demand).
+// This variant runs the same kernel with its scratch -- the membrane
+// potential of every (neuron, sample) and the barrier / error words -- in one
+// fixed array in device memory that the library reserves statically, so the
+// call itself never allocates.
+// ---------------------------------------------------------------------------
+namespace sncb {
+
+constexpr size_t kStaticScratchBytes = size_t(4) << 20;  // 4 MiB per device
+constexpr size_t kStaticCtlBytes = 256;                   // barrier counter + error word
+
+// Every device that loads the library holds this array until the process exits.
+static __device__ __align__(256) unsigned char g_bptt_static_scratch[kStaticScratchBytes];
+
+static std::mutex g_static_mu;
+static void* g_static_addr[64] = {};
+
+// Device address of the static scratch on the current device.  The host-side
+// symbol is only a stand-in for the array, not a device address, so it is
+// looked up once per device (with that device current) and cached.
+static int static_scratch(void** out) {
+  int dev = 0;
+  SNCB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    set_error("static scratch: device ordinal beyond 63");
+    return SNC_B200_EUNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (!g_static_addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_bptt_static_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_bptt_static_scratch)");
+    g_static_addr[dev] = p;
+  }
+  *out = g_static_addr[dev];
+  return SNC_B200_OK;
+}
+
+}  // namespace sncb
+
+extern "C" int snc_b200_bptt_forward_static(snc_b200_bptt* h, const float* w, const float* ext,
+                                            int32_t T, int32_t B, float threshold, float decay,
+                                            float slope, int32_t ckpt_every, int32_t smooth,
+                                            float* spikes, uint32_t* spike_bits, float* v_saved,
+                                            void* stream) {
+  using namespace sncb;
+  if (!h || !w || !ext || !spikes || !v_saved || T < 1 || B < 1 || ckpt_every < 0 ||
+      (!smooth && !spike_bits)) {
+    set_error("bptt_forward_static: bad argument");
+    return SNC_B200_EINVAL;
+  }
+  const size_t need = (size_t)h->N * (size_t)B * sizeof(float);
+  if (need > kStaticScratchBytes - kStaticCtlBytes) {
+    set_error("bptt_forward_static: num_neurons x batch = " + std::to_string((size_t)h->N * B) +
+              " exceeds the static scratch limit of " +
+              std::to_string((kStaticScratchBytes - kStaticCtlBytes) / sizeof(float)) +
+              " (use snc_b200_bptt_forward)");
+    return SNC_B200_EUNSUPPORTED;
+  }
+  void* base = nullptr;
+  int rc = static_scratch(&base);
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  unsigned* ctl = static_cast<unsigned*>(base);
+  int* err = reinterpret_cast<int*>(static_cast<char*>(base) + 16);
+  float* v = reinterpret_cast<float*>(static_cast<char*>(base) + kStaticCtlBytes);
+  BpArgs a{};
+  a.N = h->N; a.S = h->S; a.R = h->R; a.T = T; a.B = B; a.K = ckpt_every; a.smooth = smooth;
+  a.thr = threshold; a.decay = decay; a.slope = slope;
+  a.row_ptr = h->row_ptr; a.out_post = h->out_post; a.out_d = h->out_d; a.col_ptr = h->col_ptr;
+  a.in_pre = h->in_pre; a.in_d = h->in_d; a.in_eidx = h->in_eidx;
+  a.w = w; a.ext = ext; a.spikes = spikes; a.bits = spike_bits; a.vsaved = v_saved;
+  a.v = v;  // zeroed by the kernel before the first step
+  a.ctl = ctl;
+  a.err = err;
+  // the previous call's barrier count and error word must not leak into this one
+  SNCB_CUDA(cudaMemsetAsync(base, 0, kStaticCtlBytes, st));
+  if ((rc = launch(true, smooth != 0, a, h->sm_count, st))) return rc;
+  int e = 0;
+  SNCB_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SNCB_CUDA(cudaStreamSynchronize(st));
+  if (e) {
+    set_error("bptt_forward_static: device barrier timed out");
+    return e;
+  }
+  return SNC_B200_OK;
+}
