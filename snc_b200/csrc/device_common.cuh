@@ -139,6 +139,39 @@ __device__ __forceinline__ bool grid_sync(unsigned* ctr, unsigned target, int* e
   return s_ok != 0;
 }
 
+// grid_sync split in two: arrive publishes this CTA's writes and counts it
+// in; wait blocks until `target` arrivals (bounded as in grid_sync).  Work
+// between the two must not touch data other CTAs write before the barrier.
+__device__ __forceinline__ void grid_arrive(unsigned* ctr) {
+  __syncthreads();
+  if (threadIdx.x == 0) red_release_add_u32(ctr, 1u);
+}
+
+__device__ __forceinline__ bool grid_wait(unsigned* ctr, unsigned target, int* err) {
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    unsigned long long t0 = 0;
+    unsigned spins = 0;
+    while (ld_relaxed_u32(ctr) < target) {
+      if ((++spins & 255u) == 0) {
+        if (ld_volatile_i32(err) != 0) { ok = 0; break; }
+        const unsigned long long now = global_ns();
+        if (t0 == 0) t0 = now;
+        else if (now - t0 > kSpinTimeoutNs) {
+          atomicCAS(err, 0, kErrTimeout);
+          ok = 0;
+          break;
+        }
+      }
+    }
+    fence_acq_rel_gpu();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
 // Largest k in [0, n) with a[k] <= x, for a non-decreasing a with a[0] <= x.
 __device__ __forceinline__ int upper_index(const int* a, int n, int x) {
   int lo = 0, hi = n;  // invariant: a[lo] <= x, answer in [lo, hi)

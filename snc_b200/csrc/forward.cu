@@ -45,7 +45,8 @@ namespace sncb {
 
 enum { MODE_ATOMIC = 0, MODE_BUCKET = 1, MODE_SORT = 2 };
 
-constexpr int kGThreads = 512;      // tier G / plain block size
+constexpr int kGThreads = 512;      // plain-path block size; tier G minimum
+constexpr int kGThreadsMax = 768;   // tier G block size bound (one CTA per SM)
 constexpr int kGChunk = 1024;       // staged events per ordered-apply chunk
 constexpr int kGDesc = 1024;        // inbox descriptors handled per chunk
 constexpr int kMaxWave = 64;        // samples per lockstep wave
@@ -445,7 +446,7 @@ struct GSmem {
   int* rp;                   // PERSIST [BS+1] row_ptr of the block's neurons
   int* gp;                   // PERSIST [BS+1] gptr of the block's neurons
   float* ring;               // RSM [Bw][R][BS]
-  float* ext;                // [BS]
+  float* ext;                // [Bw][BS] (one drive buffer per wave slot)
   int* fired;                // [BS]
   int* pa;                   // [P+1]
   int* ib;                   // [P+1] inbox base of every destination block
@@ -463,7 +464,7 @@ struct GSmem {
 static size_t g_smem_bytes(int BS, int P, int R, int Bw, bool persist, bool rsm) {
   size_t b = 0;
   b += 8 * (size_t)kGDesc * 2;                         // desc, dsort
-  b += 4 * ((size_t)BS * 4 + 2 * (P + 1) + kGDesc + 4 * (size_t)kGChunk);
+  b += 4 * ((size_t)BS * 3 + (size_t)Bw * BS + 2 * (P + 1) + kGDesc + 4 * (size_t)kGChunk);
   if (persist) b += 4 * ((size_t)Bw * BS * 2 + BS + 2 * ((size_t)BS + 1));
   if (rsm) b += 4 * (size_t)Bw * R * BS;
   return b + 64;
@@ -476,7 +477,7 @@ __device__ __forceinline__ GSmem carve_g(unsigned char* raw, int BS, int P, int 
   s.dsort = s.desc + kGDesc;
   float* f = reinterpret_cast<float*>(s.dsort + kGDesc);
   s.ext = f;
-  s.fired = reinterpret_cast<int*>(s.ext + BS);
+  s.fired = reinterpret_cast<int*>(s.ext + (size_t)Bw * BS);
   s.head = s.fired + BS;
   s.tail = s.head + BS;
   s.pa = s.tail + BS;
@@ -499,22 +500,17 @@ __device__ __forceinline__ GSmem carve_g(unsigned char* raw, int BS, int P, int 
   return s;
 }
 
-// Phase A: drive, integrate / fire the block's neurons, publish the ascending
-// fired list, then deliver (ATOMIC) or post inbox descriptors (BUCKET, SORT).
-template <int MODE, bool PERSIST, bool RSM>
-__device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, long long* lsc, int k,
-                        int sample, long long gstep, int t, int b, int cb0) {
+// Scatter block b's share of step t's injection schedule into ext (dense
+// over the block's neurons, zero elsewhere; integration re-zeroes what it
+// reads).  Only reads the read-only inputs, so it may run between the arrival
+// at and the wait on a grid barrier.
+__device__ void load_ext(const FwdArgs& a, float* ext, int sample, long long gstep, int t, int b) {
   __shared__ int s_rng[2];
-  const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5;
-  const int nwarps = nthr >> 5;
+  const int tid = threadIdx.x, nthr = blockDim.x;
   const int lo = b * a.BS, hi = min(a.N, lo + a.BS);
-  const int R = a.R, nc = a.ncols, N = a.N, BS = a.BS, P = a.P;
-  const int par = t & 1;
-  const int s0 = t % R;
-  // this block's share of the step's injection schedule
   int k0, k1;
   if (a.sched_blk) {
-    const int* sb = a.sched_blk + gstep * (P + 1) + b;
+    const int* sb = a.sched_blk + gstep * (a.P + 1) + b;
     k0 = sb[0];
     k1 = sb[1];
   } else {
@@ -527,8 +523,25 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, long lo
     __syncthreads();
     k0 = s_rng[0];
     k1 = s_rng[1];
+    __syncthreads();
   }
-  for (int q = k0 + tid; q < k1; q += nthr) sm.ext[a.sched_nid[q] - lo] = a.sched_ext[q];
+  for (int q = k0 + tid; q < k1; q += nthr) ext[a.sched_nid[q] - lo] = a.sched_ext[q];
+}
+
+// Phase A: drive, integrate / fire the block's neurons, publish the ascending
+// fired list, then deliver (ATOMIC) or post inbox descriptors (BUCKET, SORT).
+// ext_ready: the drive of this step is already in the slot's ext buffer.
+template <int MODE, bool PERSIST, bool RSM>
+__device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, long long* lsc, int k,
+                        int sample, long long gstep, int t, int b, int cb0, bool ext_ready) {
+  const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const int nwarps = nthr >> 5;
+  const int lo = b * a.BS, hi = min(a.N, lo + a.BS);
+  const int R = a.R, nc = a.ncols, N = a.N, BS = a.BS, P = a.P;
+  const int par = t & 1;
+  const int s0 = t % R;
+  float* ext = sm.ext + (PERSIST ? (size_t)k * BS : 0);
+  if (!ext_ready) load_ext(a, ext, sample, gstep, t, b);
   __syncthreads();
   uint32_t* rast = a.raster ? a.raster + a.raster_off[sample] + (size_t)t * a.W : nullptr;
   int nf = 0;
@@ -552,8 +565,8 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, long lo
           __stcg(cell, 0.f);
         }
       }
-      const float e = sm.ext[jj];
-      sm.ext[jj] = 0.f;
+      const float e = ext[jj];
+      ext[jj] = 0.f;
       f = lif_step(a.lif, vv, rr, e, rin);
       if (PERSIST) {
         sm.v[k * BS + jj] = vv;
@@ -719,6 +732,12 @@ __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, 
   const int par = t & 1;
   const int s0 = t % R;
   int* cntp = a.inbox_cnt + ((size_t)k * 2 + par) * a.P + b;
+  const unsigned long long* box = a.inbox + ((size_t)k * 2 + par) * a.G + sm.ib[b];
+  // read the first descriptor slots in the same round trip as the count
+  // (slots beyond the count hold stale descriptors and are ignored)
+  const int cap = sm.ib[b + 1] - sm.ib[b];
+  unsigned long long spec = 0;
+  if (tid < kGDesc && tid < cap) spec = __ldcg(&box[tid]);
   if (tid == 0) {
     s_cnt = __ldcg(cntp);
     // reset for step t + 2 (written again only after the next grid barrier)
@@ -734,10 +753,9 @@ __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, 
   float* rb = ring_base<RSM>(a, sm, k);
   const int stride = RSM ? a.BS : a.ncols;
   const int col0 = RSM ? 0 : cb0;
-  const unsigned long long* box = a.inbox + ((size_t)k * 2 + par) * a.G + a.ibase[b];
   for (int d0 = 0; d0 < cnt; d0 += kGDesc) {
     const int dn = min(kGDesc, cnt - d0);
-    for (int i = tid; i < dn; i += nthr) sm.desc[i] = __ldcg(&box[d0 + i]);
+    for (int i = tid; i < dn; i += nthr) sm.desc[i] = (d0 == 0 && i == tid) ? spec : __ldcg(&box[d0 + i]);
     __syncthreads();
     const unsigned long long* src = sm.desc;
     if (MODE == MODE_SORT) {
@@ -792,7 +810,7 @@ __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, 
 }
 
 template <int MODE, bool RSM>
-__global__ void __launch_bounds__(kGThreads, 1) k_tier_g(FwdArgs a) {
+__global__ void __launch_bounds__(kGThreadsMax, 1) k_tier_g(FwdArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int scratch[40];
   __shared__ long long lscratch[40];
@@ -808,10 +826,10 @@ __global__ void __launch_bounds__(kGThreads, 1) k_tier_g(FwdArgs a) {
   unsigned target = 0;
   for (int jj = tid; jj < BS; jj += nthr) {
     sm.col[jj] = lo + jj < hi ? a.col_of[lo + jj] : -1;
-    sm.ext[jj] = 0.f;
     sm.head[jj] = -1;
     sm.tail[jj] = -1;
   }
+  for (int i = tid; i < a.Bw * BS; i += nthr) sm.ext[i] = 0.f;
   for (int jj = tid; jj <= BS; jj += nthr) {
     const int j = min(lo + jj, hi);
     sm.rp[jj] = a.row_ptr[j];
@@ -848,9 +866,16 @@ __global__ void __launch_bounds__(kGThreads, 1) k_tier_g(FwdArgs a) {
     for (int t = 0; t < Tw; ++t) {
       for (int k = 0; k < nk; ++k)
         if (t < s_T[k])
-          phase_a<MODE, true, RSM>(a, sm, scratch, lscratch, k, s_samp[k], s_gb[k] + t, t, b, cb0);
+          phase_a<MODE, true, RSM>(a, sm, scratch, lscratch, k, s_samp[k], s_gb[k] + t, t, b, cb0,
+                                   t > 0);
+      // arrive, fetch the next step's drive while the other blocks catch up,
+      // then wait
       target += nb;
-      if (!grid_sync(&a.ctl[0], target, a.err)) return;
+      grid_arrive(&a.ctl[0]);
+      for (int k = 0; k < nk; ++k)
+        if (t + 1 < s_T[k])
+          load_ext(a, sm.ext + (size_t)k * BS, s_samp[k], s_gb[k] + t + 1, t + 1, b);
+      if (!grid_wait(&a.ctl[0], target, a.err)) return;
       if (MODE != MODE_ATOMIC)
         for (int k = 0; k < nk; ++k)
           if (t < s_T[k]) phase_b<MODE, RSM>(a, sm, scratch, k, t, b, cb0, cb1);
@@ -874,7 +899,7 @@ __global__ void __launch_bounds__(kGThreads) k_plain_a(FwdArgs a, int sample, lo
   for (int i = threadIdx.x; i <= a.P; i += blockDim.x) sm.ib[i] = a.ibase[i];
   __syncthreads();
   phase_a<MODE, false, false>(a, sm, scratch, lscratch, 0, sample, gstep, t, blockIdx.x,
-                              a.colbase[blockIdx.x]);
+                              a.colbase[blockIdx.x], false);
 }
 
 template <int MODE>
@@ -886,6 +911,7 @@ __global__ void __launch_bounds__(kGThreads) k_plain_b(FwdArgs a, int t) {
     sm.head[jj] = -1;
     sm.tail[jj] = -1;
   }
+  for (int i = threadIdx.x; i <= a.P; i += blockDim.x) sm.ib[i] = a.ibase[i];
   __syncthreads();
   phase_b<MODE, false>(a, sm, scratch, 0, t, blockIdx.x, a.colbase[blockIdx.x],
                        a.colbase[blockIdx.x + 1]);
@@ -1045,10 +1071,17 @@ static GPlan plan_tier_g(const Graph* g, int B, int mode) {
   return p;
 }
 
+// Tier-G block size: one thread per neuron of the block when it fits, so the
+// integration of a step is a single pass (at least kGThreads, which the
+// descriptor prefix scan relies on).
+static int tier_g_threads(const Graph* g) {
+  return std::max(kGThreads, std::min(kGThreadsMax, (g->BS + 31) / 32 * 32));
+}
+
 template <int MODE, bool RSM>
 static int launch_tier_g(Run* r, const FwdArgs& a, size_t smem, cudaStream_t st) {
   const Graph* g = r->g;
-  const int nthr = kGThreads;
+  const int nthr = tier_g_threads(g);
   SNCB_CUDA(cudaFuncSetAttribute(k_tier_g<MODE, RSM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   SNCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tier_g<MODE, RSM>, nthr, smem));
