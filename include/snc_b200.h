@@ -140,6 +140,12 @@ int snc_b200_inputs_upload(const snc_b200_graph* g, const snc_input_event* event
 int snc_b200_inputs_release(snc_b200_inputs* in);
 /* Bytes the schedule occupies on the device (= bytes copied host to device). */
 int snc_b200_inputs_info(const snc_b200_inputs* in, int64_t* device_bytes, int64_t* entries);
+/* Copies the schedule back (no counterpart in the reference; for checking
+ * it): sched_ptr [total steps + num_samples] (sample b's step t starts at
+ * sched_ptr[stepbase_b + b + t], its closing entry follows its last step),
+ * neuron and drive [entries]: per step the driven input neurons in ascending
+ * id and their amplitudes summed in event order.  Any pointer may be NULL. */
+int snc_b200_inputs_read(const snc_b200_inputs* in, int32_t* sched_ptr, int32_t* neuron, float* drive);
 
 /* ---- run --------------------------------------------------------------------
  * Run a batch on the device without host synchronisation.  stream is a

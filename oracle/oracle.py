@@ -108,6 +108,25 @@ def forward_batched(g: SNNGraph, events, steps, lif):
             "raster": raster, "v": v}
 
 
+def schedule_merged(g: SNNGraph, events, sample: int, T: int):
+    """Per step, the driven input neurons (ascending) and their drive summed in
+    event order.  Returns (step_ptr [T+1], nid [E], ext [E])."""
+    events = np.ascontiguousarray(events, dtype=EVENT_DTYPE)
+    gs = graph_struct(g)
+    cap = max(1, int(events.shape[0]) * max(1, int(np.bincount(
+        np.asarray(g.channel)[np.asarray(g.role) == 1]).max()) if (np.asarray(g.role) == 1).any() else 1))
+    ptr = np.zeros(T + 1, np.int32)
+    nid = np.zeros(cap, np.int32)
+    ext = np.zeros(cap, np.float32)
+    f = lib().orc_schedule_merged
+    f.restype = C.c_longlong
+    n = f(C.byref(gs), _ptr(events), C.c_size_t(events.shape[0]), int(sample), int(T), _ptr(ptr),
+          _ptr(nid), _ptr(ext), C.c_longlong(cap))
+    if n < 0:
+        raise RuntimeError("orc_schedule_merged: capacity")
+    return ptr, nid[:n].copy(), ext[:n].copy()
+
+
 def eprop_batch(g: SNNGraph, w, events, steps, lif, *, trace_decay, gamma, lr, w_max,
                 train_hidden, bmat, labels, train=True, want_elig=False, fires=None,
                 want_grad=False):

@@ -152,6 +152,43 @@ static int build_schedule(const orc_graph* g, const orc_event* ev, size_t n_ev,
   return ORC_OK;
 }
 
+/* The drive run_cpu injects at each step (cpu_backend.cpp:85-95 adds every
+ * scheduled amplitude into a zeroed per-step buffer in schedule order):
+ * per step, the driven neurons in ascending id with their summed drive.
+ * step_ptr [T+1]; nid / ext hold at most cap entries.  Returns the number of
+ * entries, or -1 when cap is too small. */
+long long orc_schedule_merged(const orc_graph* g, const orc_event* ev, size_t n_ev, int sample,
+                              int T, int* step_ptr, int* nid, float* ext, long long cap) {
+  schedule sch;
+  build_schedule(g, ev, n_ev, sample, T, &sch);
+  const int N = g->num_neurons;
+  float* acc = (float*)calloc((size_t)(N > 0 ? N : 1), sizeof(float));
+  unsigned char* hit = (unsigned char*)calloc((size_t)(N > 0 ? N : 1), 1);
+  long long n = 0;
+  int fail = 0;
+  step_ptr[0] = 0;
+  for (int t = 0; t < T && !fail; ++t) {
+    for (int k = sch.step_ptr[t]; k < sch.step_ptr[t + 1]; ++k) {
+      acc[sch.nid[k]] += sch.amp[k];
+      hit[sch.nid[k]] = 1;
+    }
+    for (int i = 0; i < N; ++i)
+      if (hit[i]) {
+        if (n >= cap) { fail = 1; break; }
+        nid[n] = i;
+        ext[n] = acc[i];
+        ++n;
+        acc[i] = 0.0f;
+        hit[i] = 0;
+      }
+    step_ptr[t + 1] = (int)n;
+  }
+  free(acc);
+  free(hit);
+  free_schedule(&sch);
+  return fail ? -1 : n;
+}
+
 /* run_cpu, serial branch (src/runtime/cpu_backend.cpp:67-191).
  *  logits   [noc]           summed output spike counts per channel
  *  raster   [T][ceil(N/32)] bit j of word (t, i/32) set when neuron i fired at t

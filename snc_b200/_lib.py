@@ -52,6 +52,7 @@ SIGNATURES = {
     "snc_b200_abi_version": (C.c_int, []),
     "snc_b200_set_device": (C.c_int, [C.c_int]),
     "snc_b200_inputs_info": (C.c_int, [P, P, P]),
+    "snc_b200_inputs_read": (C.c_int, [P, P, P, P]),
     "snc_b200_last_error": (C.c_char_p, []),
     "snc_b200_graph_upload": (C.c_int, [P, P]),
     "snc_b200_graph_release": (C.c_int, [P]),

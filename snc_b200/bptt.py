@@ -18,6 +18,7 @@ encoding, embedding, readout); the spiking core runs in libsnc_b200.so.
 from __future__ import annotations
 
 import ctypes as C
+import sys
 
 import numpy as np
 import torch
@@ -82,7 +83,8 @@ class SpikingCore:
             self.h = None
 
     def __del__(self):
-        self.release()
+        if not sys.is_finalizing():  # the library may already be unloaded
+            self.release()
 
 
 class SNNFunction(torch.autograd.Function):

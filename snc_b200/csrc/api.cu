@@ -69,9 +69,11 @@ static int validate_view(const snc_graph_view* v) {
 
 static void free_graph(Graph* g) {
   if (!g) return;
+  free_oneshot(g);
   for (void* p : {(void*)g->row_ptr, (void*)g->edges, (void*)g->post, (void*)g->col_of,
                   (void*)g->out_ch, (void*)g->role, (void*)g->channel, (void*)g->colbase,
-                  (void*)g->gedges, (void*)g->gptr, (void*)g->groups, (void*)g->ibase})
+                  (void*)g->gedges, (void*)g->gptr, (void*)g->groups, (void*)g->ibase,
+                  (void*)g->chan_ptr, (void*)g->chan_ids})
     dev_free(p);
 }
 
@@ -205,137 +207,19 @@ static int upload_graph(const snc_graph_view* v, Graph* g) {
   if ((rc = dev_upload(&g->gptr, gptr.data(), gptr.size()))) return rc;
   if ((rc = dev_upload(&g->groups, groups.data(), groups.size()))) return rc;
   if ((rc = dev_upload(&g->ibase, ibase.data(), ibase.size()))) return rc;
+  if ((rc = dev_upload(&g->chan_ptr, g->chan_ptr_h.data(), g->chan_ptr_h.size()))) return rc;
+  if ((rc = dev_upload(&g->chan_ids, g->chan_ids_h.empty() ? nullptr : g->chan_ids_h.data(),
+                       g->chan_ids_h.size())))
+    return rc;
+  g->max_fan = 0;
+  for (int c = 0; c < g->nic; ++c) g->max_fan = std::max(g->max_fan, g->chan_ptr_h[c + 1] - g->chan_ptr_h[c]);
   return SNC_B200_OK;
 }
 
 // build_schedule (cpu_backend.cpp:43-65) for a batch: per (sample, step) the
 // (neuron, drive) entries sorted by neuron, each drive summed from 0.0f in
 // event order (cpu_backend.cpp:99).  ignore_sample maps every event to sample 0.
-int upload_inputs(const Graph* g, const snc_input_event* ev, size_t n_ev, int B,
-                         const int32_t* steps, bool ignore_sample, Inputs* in) {
-  if (B < 0 || (B > 0 && !steps) || (n_ev > 0 && !ev)) {
-    set_error("bad inputs arguments");
-    return SNC_B200_EINVAL;
-  }
-  in->g = g;
-  in->B = B;
-  in->steps_h.assign(steps, steps + B);
-  for (int b = 0; b < B; ++b)
-    if (steps[b] < 0) { set_error("negative step count"); return SNC_B200_EINVAL; }
-  std::vector<long long> stepbase(B + 1, 0);
-  for (int b = 0; b < B; ++b) stepbase[b + 1] = stepbase[b] + steps[b];
-  const long long TS = stepbase[B];
-  in->total_steps = TS;
-  in->Tmax = B ? *std::max_element(steps, steps + B) : 0;
-  const int W = (g->N + 31) / 32;
-  in->raster_off_h.assign(B, 0);
-  for (int b = 0; b < B; ++b) in->raster_off_h[b] = stepbase[b] * W;
-  in->raster_words = TS * W;
-  // bucket by global step, keeping event order
-  std::vector<long long> cnt(TS + 1, 0);
-  auto accept = [&](const snc_input_event& e, int& b) {
-    b = ignore_sample ? 0 : e.sample_id;
-    if (b < 0 || b >= B) return false;
-    if (e.time < 0 || e.time >= steps[b]) return false;
-    if (e.channel_id < 0 || e.channel_id >= g->nic) return false;
-    return true;
-  };
-  for (size_t k = 0; k < n_ev; ++k) {
-    int b;
-    if (!accept(ev[k], b)) continue;
-    cnt[stepbase[b] + ev[k].time + 1] += g->chan_ptr_h[ev[k].channel_id + 1] - g->chan_ptr_h[ev[k].channel_id];
-  }
-  for (long long s = 0; s < TS; ++s) cnt[s + 1] += cnt[s];
-  std::vector<int> nid(cnt[TS]);
-  std::vector<float> amp(cnt[TS]);
-  {
-    std::vector<long long> fill(cnt.begin(), cnt.end() - 1);
-    for (size_t k = 0; k < n_ev; ++k) {
-      int b;
-      if (!accept(ev[k], b)) continue;
-      const long long gs = stepbase[b] + ev[k].time;
-      for (int q = g->chan_ptr_h[ev[k].channel_id]; q < g->chan_ptr_h[ev[k].channel_id + 1]; ++q) {
-        nid[fill[gs]] = g->chan_ids_h[q];
-        amp[fill[gs]] = ev[k].amplitude;
-        ++fill[gs];
-      }
-    }
-  }
-  // per step: stable sort by neuron, then sum duplicates in order
-  std::vector<int> out_nid;
-  std::vector<float> out_ext;
-  out_nid.reserve(nid.size());
-  out_ext.reserve(nid.size());
-  std::vector<int> sptr;
-  sptr.reserve(TS + B);
-  in->sptr_off_h.assign(B, 0);
-  std::vector<int> idx;
-  for (int b = 0; b < B; ++b) {
-    in->sptr_off_h[b] = (long long)sptr.size();
-    for (int t = 0; t < steps[b]; ++t) {
-      sptr.push_back((int)out_nid.size());
-      const long long gs = stepbase[b] + t;
-      const long long k0 = cnt[gs], k1 = cnt[gs + 1];
-      idx.resize(k1 - k0);
-      std::iota(idx.begin(), idx.end(), (int)k0);
-      std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return nid[x] < nid[y]; });
-      for (size_t q = 0; q < idx.size();) {
-        const int id = nid[idx[q]];
-        float acc = 0.0f;
-        while (q < idx.size() && nid[idx[q]] == id) acc += amp[idx[q++]];
-        out_nid.push_back(id);
-        out_ext.push_back(acc);
-      }
-    }
-    sptr.push_back((int)out_nid.size());
-  }
-  if (out_nid.size() > (size_t)INT32_MAX) { set_error("schedule too large"); return SNC_B200_EUNSUPPORTED; }
-  in->n_entries = (long long)out_nid.size();
-  // samples by descending step count (longest first balances uneven lengths)
-  in->order_h.resize(B);
-  std::iota(in->order_h.begin(), in->order_h.end(), 0);
-  std::stable_sort(in->order_h.begin(), in->order_h.end(), [&](int x, int y) { return steps[x] > steps[y]; });
-  int rc;
-  if ((rc = dev_upload(&in->steps, in->steps_h.data(), (size_t)B))) return rc;
-  if ((rc = dev_upload(&in->order, in->order_h.data(), (size_t)B))) return rc;
-  if ((rc = dev_upload(&in->sptr_off, in->sptr_off_h.data(), (size_t)B))) return rc;
-  if ((rc = dev_upload(&in->sched_ptr, sptr.data(), sptr.size()))) return rc;
-  if ((rc = dev_upload(&in->sched_nid, out_nid.data(), out_nid.size()))) return rc;
-  if ((rc = dev_upload(&in->sched_ext, out_ext.data(), out_ext.size()))) return rc;
-  if ((rc = dev_upload(&in->raster_off, in->raster_off_h.data(), (size_t)B))) return rc;
-  in->stepbase_h.assign(stepbase.begin(), stepbase.begin() + B);
-  if ((rc = dev_upload(&in->stepbase, in->stepbase_h.data(), (size_t)B))) return rc;
-  // first entry of every neuron block per step, for the multi-CTA kernels
-  const long long nblk = (long long)TS * (g->P + 1);
-  if (nblk > 0 && nblk <= (64ll << 20)) {
-    std::vector<int> blk((size_t)nblk);
-    for (int b = 0; b < B; ++b)
-      for (int t = 0; t < steps[b]; ++t) {
-        const long long gs = stepbase[b] + t;
-        const int k0 = sptr[in->sptr_off_h[b] + t], k1 = sptr[in->sptr_off_h[b] + t + 1];
-        int q = k0;
-        for (int p = 0; p <= g->P; ++p) {
-          const int lo = std::min(g->N, p * g->BS);
-          while (q < k1 && out_nid[q] < lo) ++q;
-          blk[(size_t)gs * (g->P + 1) + p] = (p == g->P) ? k1 : q;
-        }
-      }
-    if ((rc = dev_upload(&in->sched_blk, blk.data(), blk.size()))) return rc;
-    in->dev_bytes += (long long)blk.size() * 4;
-  }
-  in->dev_bytes += (long long)B * (4 + 4 + 8 + 8 + 8) + (long long)sptr.size() * 4 + in->n_entries * 8;
-  return SNC_B200_OK;
-}
-
-void free_inputs(Inputs* in) {
-  if (!in) return;
-  for (void* p : {(void*)in->steps, (void*)in->order, (void*)in->sptr_off, (void*)in->sched_ptr,
-                  (void*)in->sched_nid, (void*)in->sched_ext, (void*)in->raster_off,
-                  (void*)in->stepbase, (void*)in->sched_blk})
-    dev_free(p);
-}
-
-static void free_run(Run* r) {
+void free_run(Run* r) {
   if (!r) return;
   if (r->gexec) cudaGraphExecDestroy(r->gexec);
   for (void* p : {(void*)r->counts, (void*)r->spikes, (void*)r->events, (void*)r->raster,
@@ -369,7 +253,7 @@ static int create_run(const Graph* g, const Inputs* in, int flags, Run* r) {
   return SNC_B200_OK;
 }
 
-static int fetch_run(Run* r, float* logits, int64_t* spikes, int64_t* events, uint32_t* raster,
+int fetch_run(Run* r, float* logits, int64_t* spikes, int64_t* events, uint32_t* raster,
                      float* v_final, snc_run_stats* stats) {
   const Graph* g = r->g;
   const Inputs* in = r->in;
@@ -514,6 +398,15 @@ int snc_b200_inputs_info(const snc_b200_inputs* in, int64_t* device_bytes, int64
   return SNC_B200_OK;
 }
 
+int snc_b200_inputs_read(const snc_b200_inputs* in, int32_t* sched_ptr, int32_t* neuron, float* drive) {
+  if (!in) { set_error("null inputs"); return SNC_B200_EINVAL; }
+  const size_t np = (size_t)(in->total_steps + in->B), ne = (size_t)in->n_entries;
+  if (sched_ptr && np) SNCB_CUDA(cudaMemcpy(sched_ptr, in->sched_ptr, np * 4, cudaMemcpyDeviceToHost));
+  if (neuron && ne) SNCB_CUDA(cudaMemcpy(neuron, in->sched_nid, ne * 4, cudaMemcpyDeviceToHost));
+  if (drive && ne) SNCB_CUDA(cudaMemcpy(drive, in->sched_ext, ne * 4, cudaMemcpyDeviceToHost));
+  return SNC_B200_OK;
+}
+
 int snc_b200_run_create(const snc_b200_graph* g, const snc_b200_inputs* in, int flags,
                         snc_b200_run** out) {
   if (!g || !in || !out || in->g != g) { set_error("bad run arguments"); return SNC_B200_EINVAL; }
@@ -566,14 +459,8 @@ int snc_b200_forward(const snc_b200_graph* graph, const snc_graph_view* view,
     if ((rc = snc_b200_graph_upload(view, &owned))) return rc;
     graph = owned;
   }
-  Inputs in;
-  Run r;
-  rc = upload_inputs(graph, events, n_events, 1, &num_steps, true, &in);
-  if (!rc) rc = create_run(graph, &in, 0, &r);
-  if (!rc) rc = launch_run(&r, lif, mode, SNC_B200_PATH_PLAIN, nullptr);
-  if (!rc) rc = fetch_run(&r, logits, nullptr, nullptr, nullptr, nullptr, stats);
-  free_run(&r);
-  free_inputs(&in);
+  rc = oneshot_forward(graph, events, n_events, 1, &num_steps, true, lif, mode, SNC_B200_PATH_AUTO,
+                       logits, nullptr, nullptr, stats);
   if (owned) snc_b200_graph_release(owned);
   return rc;
 }
@@ -583,15 +470,8 @@ int snc_b200_forward_batched(const snc_b200_graph* graph, const snc_input_event*
                              const snc_lif* lif, int mode, float* logits, int64_t* spikes,
                              int64_t* events_out, snc_run_stats* stats) {
   if (!graph || !lif) { set_error("null argument"); return SNC_B200_EINVAL; }
-  Inputs in;
-  Run r;
-  int rc = upload_inputs(graph, events, n_events, num_samples, steps, false, &in);
-  if (!rc) rc = create_run(graph, &in, 0, &r);
-  if (!rc) rc = launch_run(&r, lif, mode, SNC_B200_PATH_PERSISTENT, nullptr);
-  if (!rc) rc = fetch_run(&r, logits, spikes, events_out, nullptr, nullptr, stats);
-  free_run(&r);
-  free_inputs(&in);
-  return rc;
+  return oneshot_forward(graph, events, n_events, num_samples, steps, false, lif, mode,
+                         SNC_B200_PATH_PERSISTENT, logits, spikes, events_out, stats);
 }
 
 int snc_b200_autotune(const snc_b200_graph* g, const snc_b200_inputs* in, const snc_lif* lif,

@@ -46,6 +46,8 @@ inline void dev_free(void* p) {
 // ring column (col_of[j] >= 0, assigned in ascending id order); the delay
 // ring of one sample is [ring_len][ncols] floats.  Edges are packed 8 bytes:
 // x = ring column of the post | delay << 24, y = sign[pre] * weight.
+struct OneShot;
+
 struct Graph {
   int N = 0, S = 0, R = 0, ncols = 0, noc = 0, nic = 0, max_delay = 1;
   int sm_count = 0;
@@ -59,6 +61,9 @@ struct Graph {
   int* out_ch = nullptr;    // [N] output channel or -1
   uint8_t* role = nullptr;  // [N]
   int* channel = nullptr;   // [N]
+  int* chan_ptr = nullptr;  // [nic+1] input channel -> input neurons (device copy)
+  int* chan_ids = nullptr;
+  int max_fan = 0;          // most input neurons of one channel
   // block partition for the multi-CTA (grid) kernels: block b owns neurons
   // [b*BS, min(N,(b+1)*BS)) and their ring columns [colbase[b], colbase[b+1]).
   int P = 0, BS = 0;
@@ -74,6 +79,41 @@ struct Graph {
   int* ibase = nullptr;     // [P+1]
   long long signature = 0;  // autotuner cache key
   float fanin_cv = 0.f, density = 0.f;
+  mutable OneShot* oneshot = nullptr;  // workspace of the one-call forwards
+};
+
+// Byte offsets of the arrays of a schedule image (identical on host and device).
+struct SchedLayout {
+  size_t steps = 0, order = 0, sptr_off = 0, stepbase = 0, raster_off = 0, sched_ptr = 0;
+  size_t blk = 0;  // 0: no sched_blk
+  size_t nid = 0, ext = 0, n_out = 0, total = 0;
+};
+
+// Host staging buffer: pageable (a vector) or pinned (cudaHostAlloc), grown
+// on demand.
+struct HostImage {
+  bool pinned = false;
+  unsigned char* p = nullptr;
+  size_t cap = 0;
+  std::vector<unsigned char> vec;
+  explicit HostImage(bool pin = false) : pinned(pin) {}
+  HostImage(const HostImage&) = delete;
+  HostImage& operator=(const HostImage&) = delete;
+  int reserve(size_t n);
+  void release();
+  ~HostImage() { release(); }
+};
+
+// A device allocation grown on demand (contents not kept when it grows).
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  int reserve(size_t n);
+  void release();
+  ~DevBuf() { release(); }
 };
 
 struct Inputs {
@@ -94,6 +134,11 @@ struct Inputs {
   long long* raster_off = nullptr;  // [B] first raster word of sample b
   long long n_entries = 0;
   long long dev_bytes = 0;      // bytes copied to the device for this schedule
+  SchedLayout layout;
+  void* dblock = nullptr;       // the one device allocation holding every array
+  bool owns_block = true;
+  int* d_n_out = nullptr;       // device copy of n_entries
+  int* d_err = nullptr;         // schedule builder's error word (work block)
 };
 
 struct Run {
@@ -151,11 +196,38 @@ struct EpropLaunch {
   unsigned* ctl = nullptr;
 };
 
-// api.cu: the per-step injection schedule of a batch (build_schedule,
+// Per-graph workspace of snc_b200_forward / snc_b200_forward_batched.
+struct OneShot {
+  std::mutex mu;
+  HostImage img{true};
+  DevBuf keep, work;  // the schedule and the builder's work arrays
+  Inputs in;
+  Run run;
+  int B_cap = 0;
+  cudaStream_t stream = nullptr;
+};
+
+// schedule.cu: the per-step injection schedule of a batch (build_schedule,
 // cpu_backend.cpp:43-65); ignore_sample maps every event to sample 0.
+// Uploads the events of a batch and builds its schedule on the GPU in
+// stream order on `st` (keep: the schedule, work: scratch; both grown).
+int stage_inputs(const Graph* g, const snc_input_event* ev, size_t n_ev, int B, const int32_t* steps,
+                 bool ignore_sample, Inputs* in, HostImage* img, DevBuf* keep, DevBuf* work,
+                 cudaStream_t st);
+void place_schedule(Inputs* in, void* dev);
 int upload_inputs(const Graph* g, const snc_input_event* ev, size_t n_ev, int B,
                   const int32_t* steps, bool ignore_sample, Inputs* in);
 void free_inputs(Inputs* in);
+int oneshot_forward(const Graph* g, const snc_input_event* ev, size_t n_ev, int B,
+                    const int32_t* steps, bool ignore_sample, const snc_lif* lif, int mode,
+                    int path, float* logits, int64_t* spikes, int64_t* events_out,
+                    snc_run_stats* stats);
+void free_oneshot(const Graph* g);
+
+// api.cu
+int fetch_run(Run* r, float* logits, int64_t* spikes, int64_t* events, uint32_t* raster,
+              float* v_final, snc_run_stats* stats);
+void free_run(Run* r);
 
 // forward.cu
 int launch_eprop_forward(const EpropLaunch& e, cudaStream_t stream);

@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
+import sys
 
 import numpy as np
 
@@ -188,7 +189,8 @@ class CudaTrainSession:
             self.h = None
 
     def __del__(self):
-        self.release()
+        if not sys.is_finalizing():  # the library may already be unloaded
+            self.release()
 
 
 def create(g: SNNGraph, cfg: TrainConfig, batch: int, **kw) -> CudaTrainSession:

@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
+import sys
 
 import numpy as np
 
@@ -123,7 +124,8 @@ class DeviceGraph:
             self.h = None
 
     def __del__(self):
-        self.release()
+        if not sys.is_finalizing():  # the library may already be unloaded
+            self.release()
 
 
 class DeviceInputs:
@@ -148,7 +150,8 @@ class DeviceInputs:
             self.h = None
 
     def __del__(self):
-        self.release()
+        if not sys.is_finalizing():  # the library may already be unloaded
+            self.release()
 
 
 class Run:
@@ -197,7 +200,8 @@ class Run:
             self.h = None
 
     def __del__(self):
-        self.release()
+        if not sys.is_finalizing():  # the library may already be unloaded
+            self.release()
 
 
 def forward(g: SNNGraph, events, num_steps: int, lif: LIFParams, backend: str = "b200-sort",

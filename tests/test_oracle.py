@@ -134,3 +134,27 @@ def test_eprop_restatement_matches_reference_trainer(train_hidden):
     dw = out["w"] - ref["w_before"]
     assert np.abs(dw_ref).max() > 0
     np.testing.assert_allclose(dw, dw_ref, rtol=1e-4, atol=1e-6)
+
+
+def test_schedule_merged_restatement():
+    """orc_schedule_merged against a pure-Python statement of the same
+    per-step injection: drive summed in event order, neurons ascending."""
+    g = W.random_graph(31, n_in=12)
+    ev, _ = W.random_events(32, g, 3, [9, 4, 7])
+    role, chan = np.asarray(g.role), np.asarray(g.channel)
+    nic = int(chan[role == 1].max()) + 1
+    members = {c: [i for i in range(g.num_neurons) if role[i] == 1 and chan[i] == c] for c in range(nic)}
+    for b, T in enumerate([9, 4, 7]):
+        ptr, nid, ext = O.schedule_merged(g, ev, b, T)
+        k = 0
+        for t in range(T):
+            acc = {}
+            for e in ev:
+                if e["sample_id"] != b or e["time"] != t or not 0 <= e["channel_id"] < nic:
+                    continue
+                for i in members[int(e["channel_id"])]:
+                    acc[i] = np.float32(acc.get(i, np.float32(0.0)) + e["amplitude"])
+            assert ptr[t] == k and ptr[t + 1] == k + len(acc)
+            for i in sorted(acc):
+                assert nid[k] == i and ext[k].view(np.uint32) == np.float32(acc[i]).view(np.uint32)
+                k += 1
