@@ -157,21 +157,24 @@ __device__ __forceinline__ void apply_one(float* ring, int ring_stride, int col0
 // event count can be large.
 constexpr int kSerialLinkMax = 192;
 constexpr int kRegSort = 8;
+constexpr int kFirstFlag = 1 << 30;  // marks a group's first event of its column in st_col
 
 // Ordered apply of one chunk of staged events.  Staging index q is the
 // (pre, edge) order of the CPU backend.  The events were staged with their
 // block-local column st_col[q] (head / tail of every local column = -1).
 // Every ring cell must receive its contributions in increasing q.
-//  - small chunks: one warp links the events of every column into a list in
-//    staging order, 32 events per step (match.any resolves same-column lanes);
-//    one thread per column then replays its list: O(events), no sorting, and
-//    hub columns with many events in one step stay linear.
+//  - small chunks: every warp links the events of its 32-event groups
+//    (match.any: successor within the group, first event of each column
+//    flagged), then one warp joins the groups in staging order through the
+//    column tails -- one shared-memory round trip per group; one thread per
+//    column then replays its list: O(events), no sorting, and hub columns
+//    with many events in one step stay linear.
 //  - large chunks: lists are built in parallel with atomicExch (arbitrary
 //    order); each column thread loads up to kRegSort list entries into
 //    registers, sorts them there and replays them; longer lists fall back to
 //    repeated minimum selection.
 template <bool GLOBAL_RING>
-__device__ void apply_ordered(int ce, int* head, int* tail, int ncols_local, const int* st_col,
+__device__ void apply_ordered(int ce, int* head, int* tail, int ncols_local, int* st_col,
                               const int* st_slot, const float* st_w, int* st_next, float* ring,
                               int ring_stride, int col0, int serial_max) {
   __syncthreads();
@@ -219,25 +222,44 @@ __device__ void apply_ordered(int ce, int* head, int* tail, int ncols_local, con
     __syncthreads();
     return;
   }
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
+  {
+    // 1. every warp links its own 32-event groups (match.any): successor
+    //    within the group or -1, first event of each column flagged
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const unsigned below = (1u << lane) - 1u;
-    for (int g0 = 0; g0 < ce; g0 += 32) {
+    for (int g0 = warp * 32; g0 < ce; g0 += nwarps * 32) {
       const int q = g0 + lane;
       const bool valid = q < ce;
       const int c = valid ? st_col[q] : -1 - lane;
       const unsigned peers = __match_any_sync(0xffffffffu, c);
-      const unsigned lower = peers & below;
-      const bool last = (peers & ~below & ~(1u << lane)) == 0;
-      int t = -1;
-      if (valid && !lower) t = tail[c];
-      __syncwarp();
+      const unsigned higher = peers & ~below & ~(1u << lane);
       if (valid) {
-        if (lower) st_next[g0 + 31 - __clz(lower)] = q;
-        else if (t >= 0) st_next[t] = q;
-        else head[c] = q;
-        if (last) tail[c] = q;
+        st_next[q] = higher ? g0 + __ffs(higher) - 1 : -1;
+        if (!(peers & below)) st_col[q] = c | kFirstFlag;
       }
+    }
+  }
+  __syncthreads();
+  // 2. one warp joins the groups in order through the column tails
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    for (int g0 = 0; g0 < ce; g0 += 32) {
+      const int q = g0 + lane;
+      int c = 0, t = -1;
+      bool first = false, last = false;
+      if (q < ce) {
+        const int cf = st_col[q];
+        first = (cf & kFirstFlag) != 0;
+        c = cf & ~kFirstFlag;
+        last = st_next[q] < 0;
+        if (first) t = tail[c];
+      }
+      __syncwarp();
+      if (first) {
+        if (t >= 0) st_next[t] = q;
+        else head[c] = q;
+      }
+      if (last) tail[c] = q;
       __syncwarp();
     }
   }
@@ -445,6 +467,7 @@ struct GSmem {
   int* col;                  // PERSIST [BS]   ring column (global index) or -1
   int* rp;                   // PERSIST [BS+1] row_ptr of the block's neurons
   int* gp;                   // PERSIST [BS+1] gptr of the block's neurons
+  int* och;                  // PERSIST [BS]   output channel or -1
   float* ring;               // RSM [Bw][R][BS]
   float* ext;                // [Bw][BS] (one drive buffer per wave slot)
   int* fired;                // [BS]
@@ -465,7 +488,7 @@ static size_t g_smem_bytes(int BS, int P, int R, int Bw, bool persist, bool rsm)
   size_t b = 0;
   b += 8 * (size_t)kGDesc * 2;                         // desc, dsort
   b += 4 * ((size_t)BS * 3 + (size_t)Bw * BS + 2 * (P + 1) + kGDesc + 4 * (size_t)kGChunk);
-  if (persist) b += 4 * ((size_t)Bw * BS * 2 + BS + 2 * ((size_t)BS + 1));
+  if (persist) b += 4 * ((size_t)Bw * BS * 2 + 2 * (size_t)BS + 2 * ((size_t)BS + 1));
   if (rsm) b += 4 * (size_t)Bw * R * BS;
   return b + 64;
 }
@@ -494,7 +517,8 @@ __device__ __forceinline__ GSmem carve_g(unsigned char* raw, int BS, int P, int 
     s.col = s.refr + (size_t)Bw * BS;
     s.rp = s.col + BS;
     s.gp = s.rp + (BS + 1);
-    p = s.gp + (BS + 1);
+    s.och = s.gp + (BS + 1);
+    p = s.och + BS;
   }
   if (rsm) s.ring = reinterpret_cast<float*>(p);
   return s;
@@ -531,9 +555,12 @@ __device__ void load_ext(const FwdArgs& a, float* ext, int sample, long long gst
 // Phase A: drive, integrate / fire the block's neurons, publish the ascending
 // fired list, then deliver (ATOMIC) or post inbox descriptors (BUCKET, SORT).
 // ext_ready: the drive of this step is already in the slot's ext buffer.
+// acc: per-slot spike / event totals in shared memory ([0, kMaxWave) spikes,
+// [kMaxWave, 2 kMaxWave) events) that the caller adds to the sample's totals
+// once per wave; null: added to the global totals every step.
 template <int MODE, bool PERSIST, bool RSM>
-__device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, long long* lsc, int k,
-                        int sample, long long gstep, int t, int b, int cb0, bool ext_ready) {
+__device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, unsigned long long* acc,
+                        int k, int sample, long long gstep, int t, int b, int cb0, bool ext_ready) {
   const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = nthr >> 5;
   const int lo = b * a.BS, hi = min(a.N, lo + a.BS);
@@ -577,7 +604,7 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, long lo
       }
       if (f) {
         my_events += PERSIST ? sm.rp[jj + 1] - sm.rp[jj] : a.row_ptr[j + 1] - a.row_ptr[j];
-        const int oc = a.out_ch[j];
+        const int oc = PERSIST ? sm.och[jj] : a.out_ch[j];
         if (oc >= 0) atomicAdd(&a.counts[(size_t)sample * a.noc + oc], 1);
       }
     }
@@ -591,13 +618,15 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, long lo
   __syncthreads();
   int* fo = a.fired + ((size_t)k * 2 + par) * N + lo;
   for (int i = tid; i < nf; i += nthr) __stcg(&fo[i], sm.fired[i]);
-  const long long ev = block_sum_ll(my_events, lsc);
+  {
+    unsigned long long wev = (unsigned long long)my_events;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wev += __shfl_down_sync(0xffffffffu, wev, o);
+    if (lane == 0 && wev) atomicAdd(acc ? &acc[kMaxWave + k] : &a.events[sample], wev);
+  }
   if (tid == 0) {
     __stcg(&a.fired_cnt[((size_t)k * 2 + par) * P + b], nf);
-    if (nf) {
-      atomicAdd(&a.spikes[sample], (unsigned long long)nf);
-      atomicAdd(&a.events[sample], (unsigned long long)ev);
-    }
+    if (nf) atomicAdd(acc ? &acc[k] : &a.spikes[sample], (unsigned long long)nf);
   }
   if (MODE == MODE_ATOMIC) {
     float* ringk = a.ring + (size_t)k * R * nc;
@@ -758,20 +787,41 @@ __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, 
     for (int i = tid; i < dn; i += nthr) sm.desc[i] = (d0 == 0 && i == tid) ? spec : __ldcg(&box[d0 + i]);
     __syncthreads();
     const unsigned long long* src = sm.desc;
-    if (MODE == MODE_SORT) {
-      // rank sort by first edge (first edges of distinct rows are distinct)
-      for (int i = tid; i < dn; i += nthr) {
-        const unsigned long long key = sm.desc[i];
-        int r = 0;
-        for (int q = 0; q < dn; ++q) r += (sm.desc[q] >> 32) < (key >> 32);
+    int E;
+    if (dn <= 64) {
+      // few descriptors: each finds its rank (by first edge for SORT, by
+      // position for BUCKET) and its segment offset in one pass, no scan
+      __shared__ int s_E;
+      if (tid < dn) {
+        const unsigned long long key = sm.desc[tid];
+        const unsigned kf = (unsigned)(key >> 32);
+        int r = 0, off = 0;
+        for (int q = 0; q < dn; ++q) {
+          const unsigned long long o = sm.desc[q];
+          const bool lt = MODE == MODE_SORT ? (unsigned)(o >> 32) < kf : q < tid;
+          r += lt;
+          off += lt ? (int)(o & 0xffffffffu) : 0;
+        }
         sm.dsort[r] = key;
+        sm.seg_p[r] = off;
+        if (r == dn - 1) s_E = off + (int)(key & 0xffffffffu);
       }
       __syncthreads();
       src = sm.dsort;
-    }
-    // prefix of segment lengths, two descriptors per thread
-    int E;
-    {
+      E = s_E;
+    } else {
+      if (MODE == MODE_SORT) {
+        // rank sort by first edge (first edges of distinct rows are distinct)
+        for (int i = tid; i < dn; i += nthr) {
+          const unsigned long long key = sm.desc[i];
+          int r = 0;
+          for (int q = 0; q < dn; ++q) r += (sm.desc[q] >> 32) < (key >> 32);
+          sm.dsort[r] = key;
+        }
+        __syncthreads();
+        src = sm.dsort;
+      }
+      // prefix of segment lengths, two descriptors per thread
       const int i0 = 2 * tid, i1 = 2 * tid + 1;
       const int l0 = i0 < dn ? (int)(src[i0] & 0xffffffffu) : 0;
       const int l1 = i1 < dn ? (int)(src[i1] & 0xffffffffu) : 0;
@@ -813,7 +863,7 @@ template <int MODE, bool RSM>
 __global__ void __launch_bounds__(kGThreadsMax, 1) k_tier_g(FwdArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int scratch[40];
-  __shared__ long long lscratch[40];
+  __shared__ unsigned long long s_acc[2 * kMaxWave];
   __shared__ int s_samp[kMaxWave], s_T[kMaxWave];
   __shared__ long long s_gb[kMaxWave];
   const int tid = threadIdx.x, nthr = blockDim.x;
@@ -826,6 +876,7 @@ __global__ void __launch_bounds__(kGThreadsMax, 1) k_tier_g(FwdArgs a) {
   unsigned target = 0;
   for (int jj = tid; jj < BS; jj += nthr) {
     sm.col[jj] = lo + jj < hi ? a.col_of[lo + jj] : -1;
+    sm.och[jj] = lo + jj < hi ? a.out_ch[lo + jj] : -1;
     sm.head[jj] = -1;
     sm.tail[jj] = -1;
   }
@@ -845,6 +896,8 @@ __global__ void __launch_bounds__(kGThreadsMax, 1) k_tier_g(FwdArgs a) {
       s_samp[tid] = smp;
       s_T[tid] = a.steps[smp];
       s_gb[tid] = a.stepbase[smp];
+      s_acc[tid] = 0;
+      s_acc[kMaxWave + tid] = 0;
     }
     for (int i = tid; i < nk * BS; i += nthr) {
       sm.v[i] = 0.f;
@@ -866,7 +919,7 @@ __global__ void __launch_bounds__(kGThreadsMax, 1) k_tier_g(FwdArgs a) {
     for (int t = 0; t < Tw; ++t) {
       for (int k = 0; k < nk; ++k)
         if (t < s_T[k])
-          phase_a<MODE, true, RSM>(a, sm, scratch, lscratch, k, s_samp[k], s_gb[k] + t, t, b, cb0,
+          phase_a<MODE, true, RSM>(a, sm, scratch, s_acc, k, s_samp[k], s_gb[k] + t, t, b, cb0,
                                    t > 0);
       // arrive, fetch the next step's drive while the other blocks catch up,
       // then wait
@@ -879,6 +932,11 @@ __global__ void __launch_bounds__(kGThreadsMax, 1) k_tier_g(FwdArgs a) {
       if (MODE != MODE_ATOMIC)
         for (int k = 0; k < nk; ++k)
           if (t < s_T[k]) phase_b<MODE, RSM>(a, sm, scratch, k, t, b, cb0, cb1);
+    }
+    __syncthreads();
+    if (tid < nk) {
+      if (s_acc[tid]) atomicAdd(&a.spikes[s_samp[tid]], s_acc[tid]);
+      if (s_acc[kMaxWave + tid]) atomicAdd(&a.events[s_samp[tid]], s_acc[kMaxWave + tid]);
     }
     if (a.vfinal)
       for (int k = 0; k < nk; ++k)
@@ -893,12 +951,11 @@ template <int MODE>
 __global__ void __launch_bounds__(kGThreads) k_plain_a(FwdArgs a, int sample, long long gstep, int t) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int scratch[40];
-  __shared__ long long lscratch[40];
   const GSmem sm = carve_g(smem_raw, a.BS, a.P, a.R, 1, false, false);
   for (int jj = threadIdx.x; jj < a.BS; jj += blockDim.x) sm.ext[jj] = 0.f;
   for (int i = threadIdx.x; i <= a.P; i += blockDim.x) sm.ib[i] = a.ibase[i];
   __syncthreads();
-  phase_a<MODE, false, false>(a, sm, scratch, lscratch, 0, sample, gstep, t, blockIdx.x,
+  phase_a<MODE, false, false>(a, sm, scratch, nullptr, 0, sample, gstep, t, blockIdx.x,
                               a.colbase[blockIdx.x], false);
 }
 
