@@ -12,10 +12,13 @@ timesteps, CUDA-graph captured) in the delivery mode the autotuner picks.
   value  synaptic events/s, inputs and graph resident in HBM, L2 flushed
          (256 MiB write) before every timed step, CUDA-event device time.
   e2e    the same metric through snc_b200_forward_batched with host event
-         arrays: schedule build, host->device copy, run and result read-back
-         inside the timed region (wall clock).
+         arrays: host->device copy of the events, schedule build on the
+         device, run and result read-back inside the timed region (wall clock).
 Extra keys report sample-steps/s, the plain per-sample path, the
-bit-identical SORT mode and the ratio persistent / plain.
+bit-identical SORT mode and the ratio persistent / plain; `configs` the
+C1 (ff784) and C3 (audio700, uneven lengths) forwards on both paths and one
+C3 e-prop minibatch beside its CPU restatement; `bptt` the BPTT step of the
+custom kernels against the PyTorch-autograd bridge.
 
 Reference arm (--impl reference): the reference's own CPU backend (compiled
 from its sources into oracle/_ref, snc::forward with the OpenMP backend, all
@@ -203,6 +206,91 @@ def _time_cuda(fn, steps, warmup):
     t1.record()
     torch.cuda.synchronize()
     return t0.elapsed_time(t1) / steps
+
+
+def config_legs(reps=3):
+    """The other forward configurations and the e-prop update:
+    C1 (ff784: 784-256-10, 64 samples x 50 steps) and C3 (audio700: 700 input
+    channels, 1024 recurrent, 20 outputs, 256 samples of 50-1000 steps) on the
+    persistent and the plain path in ATOMIC and SORT delivery (device time,
+    best of `reps`), and one C3 e-prop minibatch (32 samples, the graph's
+    weights, forward with eligibility + weight update, SORT) beside the CPU
+    restatement of the same minibatch (one core) with the largest weight
+    difference between them."""
+    import numpy as np
+    import torch
+    from oracle import oracle as O
+    from snc_b200 import eprop as EP
+    from snc_b200 import runtime as R
+    from snc_b200 import workloads as W
+    lif = W.lif_tau20()
+    out = {}
+    for name, g, (ev, steps) in (("C1_ff784", W.ff784_graph(), W.ff784_inputs(64)),
+                                 ("C3_audio700", W.audio700_graph(), W.audio700_inputs(256))):
+        dg = R.DeviceGraph(g)
+        di = R.DeviceInputs(dg, ev, steps)
+        run = R.Run(dg, di)
+        ss = int(np.sum(steps))
+        leg = {"samples": int(len(steps)), "sample_steps": ss}
+        for m in (R.MODE_ATOMIC, R.MODE_SORT):
+            for p in (R.PATH_PERSISTENT, R.PATH_PLAIN):
+                ms = []
+                for _ in range(reps + 1):
+                    run.launch(lif, mode=m, path=p)
+                    o = run.fetch()
+                    ms.append(o["ms"])
+                best = min(ms[1:])
+                leg[f"{R.MODE_NAMES[m]}_{R.PATH_NAMES[p]}"] = {
+                    "ms": best, "events_per_s": o["total_events"] / (best / 1e3),
+                    "sample_steps_per_s": ss / (best / 1e3)}
+        leg["persistent_vs_plain_sort"] = leg["sort_plain"]["ms"] / leg["sort_persistent"]["ms"]
+        out[name] = leg
+        run.release()
+        di.release()
+        dg.release()
+    # e-prop: one C3 minibatch
+    g = W.audio700_graph()
+    ev, steps = W.audio700_inputs(32)
+    labels = np.random.default_rng(5).integers(0, g.num_output_channels, 32).astype(np.int32)
+    cfg = EP.TrainConfig(lif=lif, lr=1.0, trace_decay=0.95, mode=R.MODE_SORT)
+    # the graph's own (signed) weights: the C3 substrate's firing regime
+    sess = EP.create(g, cfg, 32, weights=np.asarray(g.weights, np.float32) *
+                     np.asarray(g.sign, np.float32)[g.pre_ids()])
+    w0 = sess.get_weights()
+    dev_ms, wall_ms = [], []
+    for i in range(reps + 1):
+        sess.set_weights(w0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        o = sess.run_batch(ev, steps, labels, train=True)
+        wall_ms.append(1e3 * (time.perf_counter() - t0))
+        dev_ms.append(o["ms"])
+    w_gpu = sess.get_weights()
+    # the same minibatch with unordered (atomic) delivery, as the reference's
+    # GPU trainer delivers
+    cfg_a = EP.TrainConfig(lif=lif, lr=1.0, trace_decay=0.95, mode=R.MODE_ATOMIC)
+    sess_a = EP.create(g, cfg_a, 32, weights=w0)
+    atomic_ms = []
+    for i in range(reps + 1):
+        sess_a.set_weights(w0)
+        atomic_ms.append(sess_a.run_batch(ev, steps, labels, train=True)["ms"])
+    sess_a.release()
+    t0 = time.perf_counter()
+    ref = O.eprop_batch(g, w0, ev, steps, lif, trace_decay=0.95, gamma=cfg.surrogate_scale,
+                        lr=cfg.lr, w_max=cfg.w_max, train_hidden=cfg.train_hidden,
+                        bmat=sess.feedback, labels=labels, train=True)
+    cpu_ms = 1e3 * (time.perf_counter() - t0)
+    diff = float(np.abs(w_gpu - ref["w"]).max() / max(1e-30, float(np.abs(ref["w"]).max())))
+    ss = int(np.sum(steps))
+    out["eprop_C3"] = {"batch": 32, "sample_steps": ss, "device_ms": min(dev_ms[1:]),
+                       "wall_ms": min(wall_ms[1:]), "synaptic_events": int(o["events"]),
+                       "events_per_s": o["events"] / (min(dev_ms[1:]) / 1e3),
+                       "device_ms_atomic_delivery": min(atomic_ms[1:]),
+                       "samples_per_s": 32 / (min(wall_ms[1:]) / 1e3),
+                       "cpu_port_ms": cpu_ms, "cpu_cores": 1,
+                       "max_rel_weight_diff": diff}
+    sess.release()
+    return out
 
 
 def bptt_leg(steps=3, warmup=2, lm=True):
@@ -408,6 +496,7 @@ def our_arm(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_extra:
         cpu = cpu_baseline(g, ev, lif)
+        extra["configs"] = config_legs()
         extra["bptt"] = bptt_leg()
 
     if rank == 0:

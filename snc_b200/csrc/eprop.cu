@@ -40,6 +40,9 @@ struct snc_b200_eprop {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int last_B = 0;
   bool have_elig = false;
+  // deferred eligibility: the forward records psi per ring column and step
+  // and the spike raster; k_elig_deferred then builds E from them
+  sncb::DevBuf psi_hist, raster;
 };
 
 namespace sncb {
@@ -110,6 +113,63 @@ __global__ void k_get_weights(int S, const uint2* edges, float* w) {
 
 static inline int grid_of(long long n, int b = 256) { return (int)std::max(1ll, (n + b - 1) / b); }
 
+// Most bytes the psi history of one minibatch may take; beyond it the
+// eligibility is accumulated inside the forward instead.
+constexpr size_t kPsiHistMax = size_t(2) << 30;
+constexpr int kEligPerLane = 4;  // synapses of one row held per lane
+
+// Eligibility of every synapse after the forward of a minibatch
+// (cuda_trainer.cu:105-112 restated per synapse): for sample b and synapse e
+// (pre i, post column c), E[b][e] = sum over t = 0..T_b-1, in step order, of
+// psi[b][c][t] * tr_i(t), with the pre trace rebuilt from the raster,
+// tr_i(t) = decay * tr_i(t-1) + (1 - decay) * fired_i(t), and every product
+// and sum rounded as the per-step update rounds it; steps whose trace is
+// exactly zero add nothing (trainer.cpp:243-244).  One warp per (sample,
+// row); each lane keeps kEligPerLane synapses of the row in registers.
+__global__ void k_elig_deferred(int B, int N, int S, const int* row_ptr, const uint2* edges,
+                                const int* steps, const long long* raster_off,
+                                const uint32_t* raster, int W, const float* psi, int nc, int psi_T,
+                                float decay, float* elig) {
+  const int lane = threadIdx.x & 31;
+  const long long nwarps_total = (long long)gridDim.x * (blockDim.x >> 5);
+  const float c1 = __fsub_rn(1.f, decay);
+  for (long long wi = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+       wi < (long long)B * N; wi += nwarps_total) {
+    const int b = (int)(wi / N), i = (int)(wi - (long long)b * N);
+    const int rs = row_ptr[i], re = row_ptr[i + 1];
+    if (rs == re) continue;
+    const int T = steps[b];
+    const uint32_t* rw = raster + raster_off[b] + (i >> 5);
+    const uint32_t bit = 1u << (i & 31);
+    const float* pb = psi + (size_t)b * nc * psi_T;
+    float* Eb = elig + (size_t)b * S;
+    for (int e0 = rs; e0 < re; e0 += 32 * kEligPerLane) {
+      const float* prow[kEligPerLane];
+      float acc[kEligPerLane];
+#pragma unroll
+      for (int k = 0; k < kEligPerLane; ++k) {
+        const int e = e0 + lane + 32 * k;
+        prow[k] = e < re ? pb + (size_t)edge_col(edges[e]) * psi_T : nullptr;
+        acc[k] = 0.f;
+      }
+      float tr = 0.f;
+      for (int t = 0; t < T; ++t) {
+        const float f = (__ldg(rw + (size_t)t * W) & bit) ? 1.f : 0.f;
+        tr = __fadd_rn(__fmul_rn(decay, tr), __fmul_rn(c1, f));
+        if (tr == 0.f) continue;
+#pragma unroll
+        for (int k = 0; k < kEligPerLane; ++k)
+          if (prow[k]) acc[k] = __fadd_rn(acc[k], __fmul_rn(__ldg(prow[k] + t), tr));
+      }
+#pragma unroll
+      for (int k = 0; k < kEligPerLane; ++k) {
+        const int e = e0 + lane + 32 * k;
+        if (e < re) Eb[e] = acc[k];
+      }
+    }
+  }
+}
+
 static void free_session(snc_b200_eprop* s) {
   for (void* p : {(void*)s->edges, (void*)s->bmat, (void*)s->internal_row, (void*)s->elig,
                   (void*)s->counts, (void*)s->delta, (void*)s->L, (void*)s->labels,
@@ -118,6 +178,8 @@ static void free_session(snc_b200_eprop* s) {
     dev_free(p);
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
+  s->psi_hist.release();
+  s->raster.release();
 }
 
 static int create_session(snc_b200_eprop* s, const Graph* g, const snc_lif* lif,
@@ -206,7 +268,18 @@ static int run_batch(snc_b200_eprop* s, const snc_input_event* ev, size_t n_ev, 
   chk(cudaMemsetAsync(s->events, 0, (size_t)B * 8, st), "memset events");
   chk(cudaMemsetAsync(s->ctl, 0, 16, st), "memset ctl");
   chk(cudaMemsetAsync(s->err, 0, 4, st), "memset err");
-  if (train) chk(cudaMemsetAsync(s->elig, 0, (size_t)B * S * sizeof(float), st), "memset elig");
+  // deferred eligibility when the psi history of this minibatch fits its budget
+  const int W = (N + 31) / 32;
+  const size_t psi_bytes = (size_t)B * std::max(1, g->ncols) * std::max(1, in.Tmax) * sizeof(float);
+  const bool deferred = train && psi_bytes <= kPsiHistMax;
+  if (deferred) {
+    if ((rc = s->psi_hist.reserve(psi_bytes))) { free_inputs(&in); return rc; }
+    if ((rc = s->raster.reserve((size_t)std::max(1ll, in.raster_words) * sizeof(uint32_t)))) {
+      free_inputs(&in);
+      return rc;
+    }
+  }
+  if (train && !deferred) chk(cudaMemsetAsync(s->elig, 0, (size_t)B * S * sizeof(float), st), "memset elig");
   if (train) {
     chk(cudaMemcpyAsync(s->labels, labels, (size_t)B * 4, cudaMemcpyHostToDevice, st), "labels");
     chk(cudaMemcpyAsync(s->steps, steps, (size_t)B * 4, cudaMemcpyHostToDevice, st), "steps");
@@ -220,8 +293,13 @@ static int run_batch(snc_b200_eprop* s, const snc_input_event* ev, size_t n_ev, 
     e.counts = s->counts;
     e.spikes = s->spikes;
     e.events = s->events;
-    e.elig = train ? s->elig : nullptr;
+    e.elig = train && !deferred ? s->elig : nullptr;
     e.fires = train ? s->fires : nullptr;
+    if (deferred) {
+      e.psi_hist = static_cast<float*>(s->psi_hist.p);
+      e.psi_T = std::max(1, in.Tmax);
+      e.raster = static_cast<uint32_t*>(s->raster.p);
+    }
     e.gamma = s->cfg.surrogate_scale;
     e.trace_decay = s->cfg.trace_decay;
     e.lif = s->lif;
@@ -230,6 +308,19 @@ static int run_batch(snc_b200_eprop* s, const snc_input_event* ev, size_t n_ev, 
     e.ctl = s->ctl;
     rc = launch_eprop_forward(e, st);
     ok = rc == SNC_B200_OK;
+    if (ok && deferred) {
+      int dev = 0, sms = 148;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      const long long warps = (long long)B * N;
+      const int blocks = (int)std::max(1ll, std::min((warps + 7) / 8, (long long)sms * 8));
+      k_elig_deferred<<<blocks, 256, 0, st>>>(B, N, S, g->row_ptr, s->edges, in.steps, in.raster_off,
+                                              static_cast<const uint32_t*>(s->raster.p), W,
+                                              static_cast<const float*>(s->psi_hist.p),
+                                              std::max(1, g->ncols), std::max(1, in.Tmax),
+                                              s->cfg.trace_decay, s->elig);
+      chk(cudaGetLastError(), "deferred eligibility");
+    }
   }
   if (ok && train) {
     bool uniform = true;

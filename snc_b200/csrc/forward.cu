@@ -98,6 +98,10 @@ struct FwdArgs {
   float* elig;
   unsigned long long* fires;
   float gamma, trace_decay;
+  // deferred eligibility: psi of every ring column and step, [B][ncols][psi_T]
+  // (null: eligibility accumulated in the forward into elig)
+  float* psi_hist;
+  int psi_T;
 };
 
 // Shared-memory bytes of the tier-S kernel for this graph.
@@ -358,7 +362,11 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
             // cuda_trainer.cu:151-153: triangular surrogate and pre trace
             const float thr = a.lif.thr;
             const float dd = __fdiv_rn(fabsf(__fsub_rn(vpre, thr)), thr > 0.f ? thr : 1.f);
-            if (c >= 0) psi[c] = dd < 1.f ? __fmul_rn(a.gamma, __fsub_rn(1.f, dd)) : 0.f;
+            if (c >= 0) {
+              const float ps = dd < 1.f ? __fmul_rn(a.gamma, __fsub_rn(1.f, dd)) : 0.f;
+              psi[c] = ps;
+              if (a.psi_hist) a.psi_hist[((size_t)b * nc + c) * a.psi_T + t] = ps;
+            }
             tr[j] = __fadd_rn(__fmul_rn(a.trace_decay, tr[j]),
                               __fmul_rn(__fsub_rn(1.f, a.trace_decay), f ? 1.f : 0.f));
             if (f && a.fires) atomicAdd(&a.fires[j], 1ull);
@@ -1096,6 +1104,8 @@ int launch_eprop_forward(const EpropLaunch& e, cudaStream_t st) {
   a.err = e.err; a.ctl = e.ctl;
   a.lif = LifP{e.lif.threshold, e.lif.decay, e.lif.reset, e.lif.refractory, e.lif.reset_mode};
   a.elig = e.elig; a.fires = e.fires; a.gamma = e.gamma; a.trace_decay = e.trace_decay;
+  a.psi_hist = e.psi_hist; a.psi_T = e.psi_T;
+  a.raster = e.raster;
   if (e.mode == MODE_SORT) return launch_tier_s_kernel<MODE_SORT, true>(g, in->B, a, st);
   return launch_tier_s_kernel<MODE_ATOMIC, true>(g, in->B, a, st);
 }

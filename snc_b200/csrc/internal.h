@@ -187,8 +187,11 @@ struct EpropLaunch {
   int* counts = nullptr;         // [B][max(1,noc)]
   unsigned long long* spikes = nullptr;
   unsigned long long* events = nullptr;
-  float* elig = nullptr;         // [B][S] (null: no eligibility)
+  float* elig = nullptr;         // [B][S] accumulated in the forward (null: none)
   unsigned long long* fires = nullptr;
+  float* psi_hist = nullptr;     // [B][ncols][psi_T] surrogate per column and step
+  int psi_T = 0;
+  uint32_t* raster = nullptr;    // spike raster, at the inputs' raster offsets
   float gamma = 0.f, trace_decay = 0.f;
   snc_lif lif{};
   int mode = 2;
