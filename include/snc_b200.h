@@ -138,6 +138,25 @@ int snc_b200_inputs_upload(const snc_b200_graph* g, const snc_input_event* event
                            size_t n_events, int32_t num_samples, const int32_t* steps,
                            snc_b200_inputs** out);
 int snc_b200_inputs_release(snc_b200_inputs* in);
+
+/* Input encoders (include/snc/encoders.hpp:14-50, src/training/encoders.cpp:25-71)
+ * run on the device: the schedule of a batch built straight from its
+ * features [num_samples][n_channels] (host, row-major), sample b spanning
+ * steps[b] steps; only the features and step counts are copied.  Encoders as
+ * the reference's enum: direct (every step, amplitude v * gain) and latency
+ * (one spike at lround((T-1) * (1 - min(1, v)))) give exactly the schedule of
+ * the reference's encode() events; poisson keeps the rule u < min(1, v *
+ * max_rate) with amplitude gain but draws u from Philox-4x32-10 (Salmon et al.,
+ * SC 2011) keyed by seed and counted by (step / 4, channel, sample): the same
+ * statistics as encode(), not the same draws.  Channels with v <= threshold
+ * emit nothing. */
+#define SNC_B200_ENCODER_DIRECT 0
+#define SNC_B200_ENCODER_POISSON 1
+#define SNC_B200_ENCODER_LATENCY 2
+int snc_b200_inputs_encode(const snc_b200_graph* g, int32_t encoder, const float* features,
+                           int32_t n_channels, int32_t num_samples, const int32_t* steps,
+                           float gain, float max_rate, float threshold, uint64_t seed,
+                           snc_b200_inputs** out);
 /* Bytes the schedule occupies on the device (= bytes copied host to device). */
 int snc_b200_inputs_info(const snc_b200_inputs* in, int64_t* device_bytes, int64_t* entries);
 /* Copies the schedule back (no counterpart in the reference; for checking

@@ -16,6 +16,7 @@ OK, EINVAL, ENODEV, ENOMEM, ECUDA, ETIMEOUT, EUNSUPPORTED, EOVERFLOW = 0, -1, -2
 MODE_ATOMIC, MODE_BUCKET, MODE_SORT, MODE_AUTO = 0, 1, 2, 3
 PATH_PLAIN, PATH_PERSISTENT, PATH_AUTO = 0, 1, 2
 RUN_RASTER, RUN_VFINAL, RUN_GRAPH, RUN_FORCE_GRID = 1, 2, 4, 8
+ENCODER_DIRECT, ENCODER_POISSON, ENCODER_LATENCY = 0, 1, 2
 
 STATUS_NAMES = {0: "OK", -1: "EINVAL", -2: "ENODEV", -3: "ENOMEM", -4: "ECUDA", -5: "ETIMEOUT",
                 -6: "EUNSUPPORTED", -7: "EOVERFLOW"}
@@ -53,6 +54,8 @@ SIGNATURES = {
     "snc_b200_set_device": (C.c_int, [C.c_int]),
     "snc_b200_inputs_info": (C.c_int, [P, P, P]),
     "snc_b200_inputs_read": (C.c_int, [P, P, P, P]),
+    "snc_b200_inputs_encode": (C.c_int, [P, I32, P, I32, I32, P, C.c_float, C.c_float, C.c_float,
+                                         C.c_uint64, P]),
     "snc_b200_last_error": (C.c_char_p, []),
     "snc_b200_graph_upload": (C.c_int, [P, P]),
     "snc_b200_graph_release": (C.c_int, [P]),

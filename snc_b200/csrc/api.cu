@@ -384,6 +384,20 @@ int snc_b200_inputs_upload(const snc_b200_graph* g, const snc_input_event* event
   return SNC_B200_OK;
 }
 
+int snc_b200_inputs_encode(const snc_b200_graph* g, int32_t encoder, const float* features,
+                           int32_t n_channels, int32_t num_samples, const int32_t* steps,
+                           float gain, float max_rate, float threshold, uint64_t seed,
+                           snc_b200_inputs** out) {
+  if (!g || !out) { set_error("null argument"); return SNC_B200_EINVAL; }
+  *out = nullptr;
+  auto* in = new snc_b200_inputs();
+  int rc = encode_inputs(g, encoder, features, n_channels, num_samples, steps, gain, max_rate,
+                         threshold, seed, in);
+  if (rc) { free_inputs(in); delete in; return rc; }
+  *out = in;
+  return SNC_B200_OK;
+}
+
 int snc_b200_inputs_release(snc_b200_inputs* in) {
   if (!in) return SNC_B200_OK;
   free_inputs(in);

@@ -214,9 +214,13 @@ struct OneShot {
 // cpu_backend.cpp:43-65); ignore_sample maps every event to sample 0.
 // Uploads the events of a batch and builds its schedule on the GPU in
 // stream order on `st` (keep: the schedule, work: scratch; both grown).
+// ev_device: the events already lie in device memory.
 int stage_inputs(const Graph* g, const snc_input_event* ev, size_t n_ev, int B, const int32_t* steps,
                  bool ignore_sample, Inputs* in, HostImage* img, DevBuf* keep, DevBuf* work,
-                 cudaStream_t st);
+                 cudaStream_t st, bool ev_device);
+// The schedule of a batch encoded on the device from its features.
+int encode_inputs(const Graph* g, int enc, const float* features, int C, int B, const int32_t* steps,
+                  float gain, float max_rate, float threshold, uint64_t seed, Inputs* in);
 void place_schedule(Inputs* in, void* dev);
 int upload_inputs(const Graph* g, const snc_input_event* ev, size_t n_ev, int B,
                   const int32_t* steps, bool ignore_sample, Inputs* in);

@@ -374,7 +374,7 @@ void DevBuf::release() {
 
 int stage_inputs(const Graph* g, const snc_input_event* ev, size_t n_ev, int B, const int32_t* steps,
                  bool ignore_sample, Inputs* in, HostImage* img, DevBuf* keep, DevBuf* work,
-                 cudaStream_t st) {
+                 cudaStream_t st, bool ev_device) {
   if (B < 0 || (B > 0 && !steps) || (n_ev > 0 && !ev)) {
     set_error("bad inputs arguments");
     return SNC_B200_EINVAL;
@@ -406,9 +406,12 @@ int stage_inputs(const Graph* g, const snc_input_event* ev, size_t n_ev, int B, 
   std::iota(in->order_h.begin(), in->order_h.end(), 0);
   std::stable_sort(in->order_h.begin(), in->order_h.end(), [&](int x, int y) { return steps[x] > steps[y]; });
   // a bound on the (event, input neuron) entries: the events themselves when
-  // every channel drives at most one neuron, else counted here
+  // every channel drives at most one neuron, else counted here (device
+  // events: every event at the largest fan-out)
   long long cap = (long long)n_ev;
-  if (g->max_fan > 1) {
+  if (g->max_fan > 1 && ev_device) {
+    cap = (long long)n_ev * g->max_fan;
+  } else if (g->max_fan > 1) {
     cap = 0;
     const int* cp = g->chan_ptr_h.data();
     for (size_t k = 0; k < n_ev; ++k) {
@@ -471,13 +474,14 @@ int stage_inputs(const Graph* g, const snc_input_event* ev, size_t n_ev, int B, 
   unsigned char* Wk = static_cast<unsigned char*>(work->p);
   place_schedule(in, K);
   SNCB_CUDA(cudaMemcpyAsync(K, h, head_bytes, cudaMemcpyHostToDevice, st));
-  if (n_ev) SNCB_CUDA(cudaMemcpyAsync(Wk + w_ev, ev, n_ev * sizeof(snc_input_event), cudaMemcpyHostToDevice, st));
+  if (n_ev && !ev_device)
+    SNCB_CUDA(cudaMemcpyAsync(Wk + w_ev, ev, n_ev * sizeof(snc_input_event), cudaMemcpyHostToDevice, st));
   SNCB_CUDA(cudaMemsetAsync(Wk + w_cnt, 0, w_zero_end - w_cnt, st));
   SNCB_CUDA(cudaMemsetAsync(Wk + w_err, 0, 4, st));
-  in->dev_bytes = (long long)(head_bytes + n_ev * sizeof(snc_input_event));
+  in->dev_bytes = (long long)(head_bytes + (ev_device ? 0 : n_ev * sizeof(snc_input_event)));
 
   SchedArgs a;
-  a.ev = reinterpret_cast<const snc_input_event*>(Wk + w_ev);
+  a.ev = ev_device ? ev : reinterpret_cast<const snc_input_event*>(Wk + w_ev);
   a.n_ev = (long long)n_ev;
   a.B = B;
   a.TS = (int)TS;
@@ -554,7 +558,7 @@ int upload_inputs(const Graph* g, const snc_input_event* ev, size_t n_ev, int B,
                   const int32_t* steps, bool ignore_sample, Inputs* in) {
   HostImage img;
   DevBuf keep, work;
-  int rc = stage_inputs(g, ev, n_ev, B, steps, ignore_sample, in, &img, &keep, &work, nullptr);
+  int rc = stage_inputs(g, ev, n_ev, B, steps, ignore_sample, in, &img, &keep, &work, nullptr, false);
   in->dblock = keep.p;
   in->owns_block = true;
   keep.p = nullptr;  // owned by `in` from here on
@@ -573,6 +577,169 @@ void free_inputs(Inputs* in) {
   if (!in) return;
   if (in->owns_block) dev_free(in->dblock);
   in->dblock = nullptr;
+}
+
+// ---- input encoders on the device --------------------------------------------
+// snc::encode (src/training/encoders.cpp:25-71) for a whole batch: events are
+// generated on the device from the features and fed to the schedule builder,
+// so only the features cross the bus.  Direct and latency equal the
+// reference's events exactly; Poisson draws its uniforms from Philox-4x32-10
+// (Salmon, Moraes, Dror and Shaw, "Parallel random numbers: as easy as 1, 2,
+// 3", SC 2011) instead of the reference's mt19937_64 stream -- the same
+// Bernoulli rule u < min(1, v * max_rate), different draws.  Counter
+// (t / 4, channel, sample, 0), key (seed low, seed high); word t % 4 of the
+// output gives u = (word >> 8) * 2^-24.
+
+namespace {
+
+struct EncArgs {
+  const float* feat;  // [B][C]
+  const int* steps;   // [B]
+  int B, C, enc;
+  float gain, max_rate, thr;
+  uint2 key;
+  int* cnt;                // [B * C] events per (sample, channel)
+  const int* off;          // [B * C + 1] their first slot
+  snc_input_event* ev;     // [off[B * C]]
+};
+
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const unsigned hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    const unsigned hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += 0x9E3779B9u;
+    k.y += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// Events of one (sample, channel); writes them to out when it is non-null.
+__device__ int encode_one(const EncArgs& a, int b, int c, snc_input_event* out) {
+  const int T = a.steps[b];
+  const float v = a.feat[(size_t)b * a.C + c];
+  if (!(v > a.thr) || T <= 0) return 0;
+  if (a.enc == SNC_B200_ENCODER_DIRECT) {
+    if (out) {
+      const float amp = __fmul_rn(v, a.gain);
+      for (int t = 0; t < T; ++t) out[t] = snc_input_event{b, c, t, amp};
+    }
+    return T;
+  }
+  if (a.enc == SNC_B200_ENCODER_LATENCY) {
+    const float vc = fminf(1.f, v);
+    const float x = __fmul_rn((float)(T - 1), __fsub_rn(1.f, vc));
+    int t = (int)floor((double)x + 0.5);  // lround of a non-negative float
+    t = min(max(t, 0), T - 1);
+    if (out) out[0] = snc_input_event{b, c, t, a.gain};
+    return 1;
+  }
+  const float prob = fminf(1.f, __fmul_rn(v, a.max_rate));
+  int n = 0;
+  for (int q = 0; 4 * q < T; ++q) {
+    const uint4 w = philox4x32_10(make_uint4((unsigned)q, (unsigned)c, (unsigned)b, 0u), a.key);
+    const unsigned ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int t = 4 * q + j;
+      if (t < T && (float)(ws[j] >> 8) * (1.f / 16777216.f) < prob) {
+        if (out) out[n] = snc_input_event{b, c, t, a.gain};
+        ++n;
+      }
+    }
+  }
+  return n;
+}
+
+__global__ void k_enc_count(EncArgs a) {
+  const long long n = (long long)a.B * a.C;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    a.cnt[i] = encode_one(a, (int)(i / a.C), (int)(i % a.C), nullptr);
+}
+
+__global__ void k_enc_write(EncArgs a) {
+  const long long n = (long long)a.B * a.C;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    encode_one(a, (int)(i / a.C), (int)(i % a.C), a.ev + a.off[i]);
+}
+
+}  // namespace
+
+int encode_inputs(const Graph* g, int enc, const float* features, int C, int B, const int32_t* steps,
+                  float gain, float max_rate, float threshold, uint64_t seed, Inputs* in) {
+  if (enc < SNC_B200_ENCODER_DIRECT || enc > SNC_B200_ENCODER_LATENCY || C < 0 || B < 0 ||
+      (B > 0 && !steps) || ((long long)B * C > 0 && !features)) {
+    set_error("encode: bad arguments");
+    return SNC_B200_EINVAL;
+  }
+  long long bound = 0;  // events at most: every step of every (sample, channel)
+  for (int b = 0; b < B; ++b) {
+    if (steps[b] < 0) { set_error("negative step count"); return SNC_B200_EINVAL; }
+    bound += (long long)C * steps[b];
+  }
+  if (bound > (long long)INT32_MAX) { set_error("encode: more than 2^31 possible events"); return SNC_B200_EUNSUPPORTED; }
+  const long long nbc = (long long)B * C;
+  DevBuf encw;
+  size_t w = 0;
+  const size_t w_feat = w;  w = align_up(w + (size_t)std::max(1ll, nbc) * 4);
+  const size_t w_steps = w; w = align_up(w + (size_t)std::max(1, B) * 4);
+  const size_t w_cnt = w;   w = align_up(w + (size_t)std::max(1ll, nbc) * 4);
+  const size_t w_off = w;   w = align_up(w + (size_t)(nbc + 1) * 4);
+  const size_t w_scan = w;  w = align_up(w + scan_scratch_ints(nbc) * 4);
+  int rc;
+  if ((rc = encw.reserve(w))) return rc;
+  unsigned char* E = static_cast<unsigned char*>(encw.p);
+  if (nbc) SNCB_CUDA(cudaMemcpy(E + w_feat, features, (size_t)nbc * 4, cudaMemcpyHostToDevice));
+  if (B) SNCB_CUDA(cudaMemcpy(E + w_steps, steps, (size_t)B * 4, cudaMemcpyHostToDevice));
+  EncArgs a;
+  a.feat = reinterpret_cast<const float*>(E + w_feat);
+  a.steps = reinterpret_cast<const int*>(E + w_steps);
+  a.B = B;
+  a.C = C;
+  a.enc = enc;
+  a.gain = gain;
+  a.max_rate = max_rate;
+  a.thr = threshold;
+  a.key = make_uint2((unsigned)(seed & 0xFFFFFFFFull), (unsigned)(seed >> 32));
+  a.cnt = reinterpret_cast<int*>(E + w_cnt);
+  a.off = reinterpret_cast<const int*>(E + w_off);
+  a.ev = nullptr;
+  const int sms = std::max(1, g->sm_count);
+  const unsigned grid = (unsigned)std::max(1ll, std::min((nbc + 255) / 256, (long long)sms * 8));
+  if (nbc) {
+    k_enc_count<<<grid, 256>>>(a);
+    SNCB_CUDA(cudaGetLastError());
+  }
+  if ((rc = scan_exclusive(a.cnt, reinterpret_cast<int*>(E + w_off), nbc, reinterpret_cast<int*>(E + w_scan), nullptr)))
+    return rc;
+  int n_ev = 0;
+  SNCB_CUDA(cudaMemcpy(&n_ev, E + w_off + (size_t)nbc * 4, 4, cudaMemcpyDeviceToHost));
+  DevBuf evbuf;
+  if ((rc = evbuf.reserve((size_t)std::max(1, n_ev) * sizeof(snc_input_event)))) return rc;
+  a.ev = static_cast<snc_input_event*>(evbuf.p);
+  if (n_ev) {
+    k_enc_write<<<grid, 256>>>(a);
+    SNCB_CUDA(cudaGetLastError());
+  }
+  HostImage img;
+  DevBuf keep, work;
+  rc = stage_inputs(g, a.ev, (size_t)n_ev, B, steps, false, in, &img, &keep, &work, nullptr, true);
+  in->dblock = keep.p;
+  in->owns_block = true;
+  keep.p = nullptr;
+  keep.cap = 0;
+  if (rc) return rc;
+  int host[2] = {0, 0};
+  SNCB_CUDA(cudaMemcpy(&host[0], in->d_err, 4, cudaMemcpyDeviceToHost));
+  SNCB_CUDA(cudaMemcpy(&host[1], in->d_n_out, 4, cudaMemcpyDeviceToHost));
+  in->d_err = nullptr;
+  if (host[0]) { set_error("schedule entries exceeded their bound"); return SNC_B200_EOVERFLOW; }
+  in->n_entries = host[1];
+  in->dev_bytes += (long long)nbc * 4 + (long long)B * 4;  // plus the features and step counts
+  return SNC_B200_OK;
 }
 
 // ---- one-call forward workspace ---------------------------------------------
@@ -601,7 +768,7 @@ int oneshot_forward(const Graph* g, const snc_input_event* ev, size_t n_ev, int 
   Inputs& in = ws->in;
   in.owns_block = false;
   if ((rc = stage_inputs(g, ev, n_ev, B, steps, ignore_sample, &in, &ws->img, &ws->keep, &ws->work,
-                         ws->stream)))
+                         ws->stream, false)))
     return rc;
   in.dblock = ws->keep.p;
   Run& r = ws->run;

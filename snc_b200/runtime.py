@@ -140,9 +140,49 @@ class DeviceInputs:
         check(lib().snc_b200_inputs_upload(dg.h, ptr(ev), ev.shape[0], self.B, ptr(self.steps),
                                            C.byref(h)), "inputs_upload")
         self.h = h
+        self._info()
+
+    def _info(self):
         nb, ne = C.c_int64(), C.c_int64()
         check(lib().snc_b200_inputs_info(self.h, C.byref(nb), C.byref(ne)), "inputs_info")
         self.device_bytes, self.entries = nb.value, ne.value
+
+    ENCODERS = {"direct": _lib.ENCODER_DIRECT, "poisson": _lib.ENCODER_POISSON,
+                "latency": _lib.ENCODER_LATENCY}
+
+    @classmethod
+    def encode(cls, dg: DeviceGraph, features, steps, encoder="poisson", gain=1.0, max_rate=0.5,
+               threshold=0.0, seed=1) -> "DeviceInputs":
+        """The schedule of a batch encoded on the device from its features
+        [B, n_channels] (snc_b200_inputs_encode; encoders.cpp:25-71): direct
+        and latency exactly as the reference encodes, poisson with
+        Philox-4x32-10 draws."""
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        if f.ndim != 2:
+            raise ValueError("features must be [num_samples, n_channels]")
+        self = cls.__new__(cls)
+        self.steps = np.ascontiguousarray(steps, dtype=np.int32).reshape(-1)
+        self.B = int(self.steps.shape[0])
+        if f.shape[0] != self.B:
+            raise ValueError("one row of features per sample")
+        self.dg = dg
+        enc = cls.ENCODERS[encoder] if isinstance(encoder, str) else int(encoder)
+        h = C.c_void_p()
+        check(lib().snc_b200_inputs_encode(dg.h, enc, ptr(f), f.shape[1], self.B, ptr(self.steps),
+                                           gain, max_rate, threshold, int(seed), C.byref(h)),
+              "inputs_encode")
+        self.h = h
+        self._info()
+        return self
+
+    def read(self):
+        """The schedule back on the host: (sched_ptr [total steps + B],
+        neuron [entries], drive [entries]) (snc_b200_inputs_read)."""
+        ptr_ = np.zeros(int(self.steps.sum()) + self.B, np.int32)
+        nid = np.zeros(max(1, self.entries), np.int32)
+        ext = np.zeros(max(1, self.entries), np.float32)
+        check(lib().snc_b200_inputs_read(self.h, ptr(ptr_), ptr(nid), ptr(ext)), "inputs_read")
+        return ptr_, nid[:self.entries], ext[:self.entries]
 
     def release(self):
         if getattr(self, "h", None):

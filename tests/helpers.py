@@ -40,3 +40,26 @@ def spike_count_agreement(a, b):
     if max(a, b) == 0:
         return 1.0
     return min(a, b) / max(a, b)
+
+
+def input_graph(n_in, n_hid=40, fan=1, seed=0):
+    """n_in input neurons, `fan` of them per channel (ascending ids), a few
+    hidden neurons and one output, sparse random edges."""
+    rng = np.random.default_rng(seed)
+    N = n_in + n_hid + 1
+    pre = rng.integers(0, N - 1, 4 * N)
+    post = rng.integers(n_in, N, 4 * N)
+    order = np.argsort(pre, kind="stable")
+    pre, post = pre[order], post[order]
+    row_ptr = np.zeros(N + 1, np.int64)
+    np.cumsum(np.bincount(pre, minlength=N), out=row_ptr[1:])
+    role = np.zeros(N, np.uint8)
+    role[:n_in] = 1
+    role[-1] = 2
+    channel = np.full(N, -1, np.int32)
+    channel[:n_in] = np.arange(n_in) // fan
+    channel[-1] = 0
+    return SNNGraph(N, row_ptr.astype(np.int32), post.astype(np.int32),
+                    rng.uniform(0.1, 0.5, pre.shape[0]).astype(np.float32),
+                    rng.integers(1, 5, pre.shape[0]).astype(np.int32), role,
+                    np.ones(N, np.int8), channel)

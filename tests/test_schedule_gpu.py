@@ -16,32 +16,10 @@ import pytest
 from oracle import oracle as O
 from snc_b200 import _lib
 from snc_b200 import runtime as R
-from snc_b200.graph import EVENT_DTYPE, SNNGraph
+from snc_b200.graph import EVENT_DTYPE
+from tests.helpers import input_graph as _graph
 
 pytestmark = pytest.mark.gpu
-
-
-def _graph(n_in, n_hid=40, fan=1, seed=0):
-    """n_in input neurons, `fan` of them per channel (ascending ids), a few
-    hidden neurons and one output, sparse random edges."""
-    rng = np.random.default_rng(seed)
-    N = n_in + n_hid + 1
-    pre = rng.integers(0, N - 1, 4 * N)
-    post = rng.integers(n_in, N, 4 * N)
-    order = np.argsort(pre, kind="stable")
-    pre, post = pre[order], post[order]
-    row_ptr = np.zeros(N + 1, np.int64)
-    np.cumsum(np.bincount(pre, minlength=N), out=row_ptr[1:])
-    role = np.zeros(N, np.uint8)
-    role[:n_in] = 1
-    role[-1] = 2
-    channel = np.full(N, -1, np.int32)
-    channel[:n_in] = np.arange(n_in) // fan
-    channel[-1] = 0
-    return SNNGraph(N, row_ptr.astype(np.int32), post.astype(np.int32),
-                    rng.uniform(0.1, 0.5, pre.shape[0]).astype(np.float32),
-                    rng.integers(1, 5, pre.shape[0]).astype(np.int32), role,
-                    np.ones(N, np.int8), channel)
 
 
 def _read(dg, ev, steps):
