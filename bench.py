@@ -248,6 +248,36 @@ def config_legs(reps=3):
         run.release()
         di.release()
         dg.release()
+    # input encoding of the C3 batch (256 samples x 700 channels, Poisson):
+    # on the device from the features vs the reference's encode() on the host
+    # followed by the upload of its events (both build the device schedule)
+    g = W.audio700_graph()
+    _, steps = W.audio700_inputs(256)
+    feats = np.minimum(np.random.default_rng(3).lognormal(np.log(0.01) - 0.5, 1.0, (256, 700)),
+                       1.0).astype(np.float32)
+    dg = R.DeviceGraph(g)
+    dev = []
+    for _ in range(reps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        di = R.DeviceInputs.encode(dg, feats, steps, encoder="poisson", max_rate=1.0, seed=1)
+        dev.append(1e3 * (time.perf_counter() - t0))
+        n_dev = di.entries
+        di.release()
+    leg = {"samples": 256, "channels": 700, "sample_steps": int(np.sum(steps)),
+           "device_ms": min(dev[1:]), "entries": int(n_dev)}
+    if O.ref_available():
+        t0 = time.perf_counter()
+        ev = np.concatenate([O.ref_encode("poisson", feats[b], int(steps[b]), max_rate=1.0,
+                                          seed=1 + b, sample_id=b) for b in range(256)])
+        t1 = time.perf_counter()
+        di = R.DeviceInputs(dg, ev, steps)
+        t2 = time.perf_counter()
+        leg.update({"host_encode_ms": 1e3 * (t1 - t0), "host_upload_ms": 1e3 * (t2 - t1),
+                    "host_entries": int(di.entries)})
+        di.release()
+    out["encode_C3"] = leg
+    dg.release()
     # e-prop: one C3 minibatch
     g = W.audio700_graph()
     ev, steps = W.audio700_inputs(32)
