@@ -128,6 +128,15 @@ int snc_b200_graph_release(snc_b200_graph* g);
 /* Basic shape: N, S, ring length, output channels, input channels. */
 int snc_b200_graph_info(const snc_b200_graph* g, int32_t* n, int32_t* s, int32_t* ring_len,
                         int32_t* n_out, int32_t* n_in);
+/* Copies the device layout of an uploaded graph back (no counterpart in the
+ * reference; for checking it): edges and gedges [S] as (ring column | delay
+ * << 24, float bits of sign * weight) pairs, gptr [N+1], groups [G] as
+ * (destination block, first gedge) pairs, col_of [N], colbase and ibase
+ * [P+1]; block_size and num_blocks receive BS and P, num_groups G.  Any
+ * pointer may be NULL. */
+int snc_b200_graph_layout(const snc_b200_graph* g, uint32_t* edges, uint32_t* gedges, int32_t* gptr,
+                          int32_t* groups, int32_t* col_of, int32_t* colbase, int32_t* ibase,
+                          int32_t* block_size, int32_t* num_blocks, int32_t* num_groups);
 
 /* ---- inputs ----------------------------------------------------------------
  * Build the per-step injection schedule of a batch of samples on the host

@@ -60,6 +60,7 @@ SIGNATURES = {
     "snc_b200_graph_upload": (C.c_int, [P, P]),
     "snc_b200_graph_release": (C.c_int, [P]),
     "snc_b200_graph_info": (C.c_int, [P, P, P, P, P, P]),
+    "snc_b200_graph_layout": (C.c_int, [P] * 11),
     "snc_b200_inputs_upload": (C.c_int, [P, P, C.c_size_t, I32, P, P]),
     "snc_b200_inputs_release": (C.c_int, [P]),
     "snc_b200_run_create": (C.c_int, [P, P, C.c_int, P]),

@@ -27,6 +27,8 @@ import torch.nn as nn
 from . import _lib
 from ._lib import check, lib
 
+_FINALIZING = sys.is_finalizing  # kept: module globals are cleared at exit
+
 
 def _ptr(t):
     return C.c_void_p(t.data_ptr()) if t is not None else None
@@ -83,7 +85,7 @@ class SpikingCore:
             self.h = None
 
     def __del__(self):
-        if not sys.is_finalizing():  # the library may already be unloaded
+        if not _FINALIZING():  # the library may already be unloaded
             self.release()
 
 

@@ -122,17 +122,6 @@ static int upload_graph(const snc_graph_view* v, Graph* g) {
   for (int i = 0; i < n; ++i)
     if (v->role[i] == 2 && v->channel[i] >= 0) out_ch[i] = v->channel[i];
   g->row_ptr_h.assign(v->row_ptr, v->row_ptr + n + 1);
-  // packed edges, CSR order (+2 zero entries so 128-bit loads stay in bounds)
-  std::vector<uint2> edges((size_t)m + 2, make_uint2(0, 0));
-  for (int i = 0; i < n; ++i) {
-    const float sg = static_cast<float>(v->sign[i]);
-    for (int e = v->row_ptr[i]; e < v->row_ptr[i + 1]; ++e) {
-      const float w = sg * v->weights[e];
-      uint32_t wb;
-      std::memcpy(&wb, &w, 4);
-      edges[e] = make_uint2((uint32_t)g->col_of_h[v->post_ids[e]] | ((uint32_t)v->delays[e] << 24), wb);
-    }
-  }
   // block partition for the grid kernels
   const int sm = std::max(1, g->sm_count);
   int BS = (n + sm - 1) / sm;
@@ -151,37 +140,6 @@ static int upload_graph(const snc_graph_view* v, Graph* g) {
     }
     colbase[P] = c;
   }
-  // dest-grouped edges: stable regroup of each row by destination block
-  std::vector<uint2> gedges((size_t)m + 2, make_uint2(0, 0));
-  std::vector<int> gptr(n + 1, 0);
-  std::vector<int2> groups;
-  groups.reserve((size_t)n * 4 + 1);
-  {
-    std::vector<int> idx;
-    for (int i = 0; i < n; ++i) {
-      const int rs = v->row_ptr[i], re = v->row_ptr[i + 1];
-      idx.resize(re - rs);
-      std::iota(idx.begin(), idx.end(), rs);
-      std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
-        return v->post_ids[a] / BS < v->post_ids[b] / BS;
-      });
-      int last_blk = -1;
-      for (int q = 0; q < re - rs; ++q) {
-        const int e = idx[q];
-        gedges[rs + q] = edges[e];
-        const int blk = v->post_ids[e] / BS;
-        if (blk != last_blk) {
-          groups.push_back(make_int2(blk, rs + q));
-          last_blk = blk;
-        }
-      }
-      gptr[i + 1] = (int)groups.size();
-    }
-  }
-  std::vector<int> ibase(P + 1, 0);
-  for (const int2& gr : groups) ibase[gr.x + 1]++;
-  for (int b = 0; b < P; ++b) ibase[b + 1] += ibase[b];
-  g->G = (int)groups.size();
   // fan-in skew and density for the autotuner signature
   {
     double mean = n ? (double)m / n : 0.0, var = 0.0;
@@ -194,19 +152,12 @@ static int upload_graph(const snc_graph_view* v, Graph* g) {
   }
   std::vector<uint8_t> role(v->role, v->role + n);
   std::vector<int> channel(v->channel, v->channel + n);
-  std::vector<int> post(v->post_ids, v->post_ids + m);
-  if ((rc = dev_upload(&g->row_ptr, v->row_ptr, (size_t)n + 1))) return rc;
-  if ((rc = dev_upload(&g->edges, edges.data(), edges.size()))) return rc;
-  if ((rc = dev_upload(&g->post, post.data(), post.size()))) return rc;
-  if ((rc = dev_upload(&g->col_of, g->col_of_h.data(), (size_t)n))) return rc;
+  // packed and destination-grouped edges, groups, inbox bases: on the device
+  if ((rc = build_graph_device(v, g))) return rc;
   if ((rc = dev_upload(&g->out_ch, out_ch.data(), (size_t)n))) return rc;
   if ((rc = dev_upload(&g->role, role.data(), role.size()))) return rc;
   if ((rc = dev_upload(&g->channel, channel.data(), channel.size()))) return rc;
   if ((rc = dev_upload(&g->colbase, colbase.data(), colbase.size()))) return rc;
-  if ((rc = dev_upload(&g->gedges, gedges.data(), gedges.size()))) return rc;
-  if ((rc = dev_upload(&g->gptr, gptr.data(), gptr.size()))) return rc;
-  if ((rc = dev_upload(&g->groups, groups.data(), groups.size()))) return rc;
-  if ((rc = dev_upload(&g->ibase, ibase.data(), ibase.size()))) return rc;
   if ((rc = dev_upload(&g->chan_ptr, g->chan_ptr_h.data(), g->chan_ptr_h.size()))) return rc;
   if ((rc = dev_upload(&g->chan_ids, g->chan_ids_h.empty() ? nullptr : g->chan_ids_h.data(),
                        g->chan_ids_h.size())))
@@ -370,6 +321,24 @@ int snc_b200_graph_info(const snc_b200_graph* g, int32_t* n, int32_t* s, int32_t
   if (ring_len) *ring_len = g->R;
   if (n_out) *n_out = g->noc;
   if (n_in) *n_in = g->nic;
+  return SNC_B200_OK;
+}
+
+int snc_b200_graph_layout(const snc_b200_graph* g, uint32_t* edges, uint32_t* gedges, int32_t* gptr,
+                          int32_t* groups, int32_t* col_of, int32_t* colbase, int32_t* ibase,
+                          int32_t* block_size, int32_t* num_blocks, int32_t* num_groups) {
+  if (!g) { set_error("null graph"); return SNC_B200_EINVAL; }
+  const size_t S = (size_t)g->S, N = (size_t)g->N, P = (size_t)g->P, G = (size_t)g->G;
+  if (edges && S) SNCB_CUDA(cudaMemcpy(edges, g->edges, S * 8, cudaMemcpyDeviceToHost));
+  if (gedges && S) SNCB_CUDA(cudaMemcpy(gedges, g->gedges, S * 8, cudaMemcpyDeviceToHost));
+  if (gptr) SNCB_CUDA(cudaMemcpy(gptr, g->gptr, (N + 1) * 4, cudaMemcpyDeviceToHost));
+  if (groups && G) SNCB_CUDA(cudaMemcpy(groups, g->groups, G * 8, cudaMemcpyDeviceToHost));
+  if (col_of && N) SNCB_CUDA(cudaMemcpy(col_of, g->col_of, N * 4, cudaMemcpyDeviceToHost));
+  if (colbase) SNCB_CUDA(cudaMemcpy(colbase, g->colbase, (P + 1) * 4, cudaMemcpyDeviceToHost));
+  if (ibase) SNCB_CUDA(cudaMemcpy(ibase, g->ibase, (P + 1) * 4, cudaMemcpyDeviceToHost));
+  if (block_size) *block_size = g->BS;
+  if (num_blocks) *num_blocks = g->P;
+  if (num_groups) *num_groups = g->G;
   return SNC_B200_OK;
 }
 

@@ -218,6 +218,13 @@ struct OneShot {
 int stage_inputs(const Graph* g, const snc_input_event* ev, size_t n_ev, int B, const int32_t* steps,
                  bool ignore_sample, Inputs* in, HostImage* img, DevBuf* keep, DevBuf* work,
                  cudaStream_t st, bool ev_device);
+// Exclusive prefix sums of int counts on the device (totals < 2^31): out[0..n]
+// from in[0..n) in stream order; scratch holds scan_scratch_ints(n) ints.
+size_t scan_scratch_ints(long long n);
+int scan_exclusive(const int* in, int* out, long long n, int* scratch, cudaStream_t st);
+// graphbuild.cu: packed and destination-grouped edges, groups and inbox
+// bases of a validated graph, built on the device (g->N, S, BS, P, col_of_h set).
+int build_graph_device(const snc_graph_view* v, Graph* g);
 // The schedule of a batch encoded on the device from its features.
 int encode_inputs(const Graph* g, int enc, const float* features, int C, int B, const int32_t* steps,
                   float gain, float max_rate, float threshold, uint64_t seed, Inputs* in);

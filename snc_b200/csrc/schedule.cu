@@ -86,6 +86,8 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_add(int* out, long long n
   if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = bex[gridDim.x];
 }
 
+}  // namespace
+
 // Ints of scratch scan_exclusive needs for n items.
 size_t scan_scratch_ints(long long n) {
   size_t s = 0;
@@ -110,6 +112,8 @@ int scan_exclusive(const int* in, int* out, long long n, int* scratch, cudaStrea
   SNCB_CUDA(cudaGetLastError());
   return SNC_B200_OK;
 }
+
+namespace {
 
 // ---- schedule kernels ----------------------------------------------------------
 

@@ -24,6 +24,8 @@ from ._lib import check, lib, ptr
 from .graph import INTERNAL, SNNGraph
 from .runtime import DeviceGraph, LIFParams, _events
 
+_FINALIZING = sys.is_finalizing  # kept: module globals are cleared at exit
+
 
 class EpropCfg(C.Structure):
     _fields_ = [("lr", C.c_float), ("w_max", C.c_float), ("surrogate_scale", C.c_float),
@@ -189,7 +191,7 @@ class CudaTrainSession:
             self.h = None
 
     def __del__(self):
-        if not sys.is_finalizing():  # the library may already be unloaded
+        if not _FINALIZING():  # the library may already be unloaded
             self.release()
 
 

@@ -12,8 +12,9 @@ Mirrors include/snc/runtime.hpp:
   * ``LIFParams`` (runtime.hpp:34-39) plus ``reset_mode`` (1 = subtractive).
   * ``RunStats`` / ``ForwardResult`` (runtime.hpp:41-52).
   * ``forward(g, events, num_steps, lif, backend)`` (runtime.hpp:57-58): one
-    sample through the plain per-sample path.  Unlike the reference, an
-    unavailable device raises instead of silently falling back to the CPU.
+    sample through the autotuned path (persistent unless the tuner chose the
+    plain per-step launches).  Unlike the reference, an unavailable device
+    raises instead of silently falling back to the CPU.
 
 Batched execution, device-resident inputs and results, and the autotuner are
 additions: ``DeviceGraph``, ``DeviceInputs``, ``Run``, ``forward_batched``.
@@ -31,6 +32,8 @@ from ._lib import (MODE_ATOMIC, MODE_AUTO, MODE_BUCKET, MODE_SORT, PATH_AUTO, PA
                    PATH_PLAIN, RUN_FORCE_GRID, RUN_GRAPH, RUN_RASTER, RUN_VFINAL, check, lib,
                    ptr)
 from .graph import EVENT_DTYPE, SNNGraph
+
+_FINALIZING = sys.is_finalizing  # kept: module globals are cleared at exit
 
 BACKENDS = {
     "cuda-atomic": MODE_ATOMIC, "cuda-bucket": MODE_BUCKET, "cuda-sort": MODE_SORT,
@@ -124,7 +127,7 @@ class DeviceGraph:
             self.h = None
 
     def __del__(self):
-        if not sys.is_finalizing():  # the library may already be unloaded
+        if not _FINALIZING():  # the library may already be unloaded
             self.release()
 
 
@@ -190,7 +193,7 @@ class DeviceInputs:
             self.h = None
 
     def __del__(self):
-        if not sys.is_finalizing():  # the library may already be unloaded
+        if not _FINALIZING():  # the library may already be unloaded
             self.release()
 
 
@@ -240,7 +243,7 @@ class Run:
             self.h = None
 
     def __del__(self):
-        if not sys.is_finalizing():  # the library may already be unloaded
+        if not _FINALIZING():  # the library may already be unloaded
             self.release()
 
 
