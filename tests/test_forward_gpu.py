@@ -159,3 +159,21 @@ def test_batched_one_call_and_autotune():
     run.launch(lif, mode=R.MODE_AUTO, path=R.PATH_AUTO)
     run.fetch()
     assert run.used() == (best["mode"], best["path"])
+
+
+@pytest.mark.parametrize("pname,path,force", PATHS)
+def test_sort_bit_exact_at_the_largest_delay(pname, path, force):
+    # delays up to 255 (the backend's limit; 8 bits in the packed edge): a
+    # 256-slot ring, slots that wrap many times over 600 steps
+    g = W.random_graph(17, n_hid=90, max_delay=6)
+    rng = np.random.default_rng(17)
+    d = g.delays.copy()
+    d[rng.random(d.shape[0]) < 0.3] = 255
+    d[::7] = rng.integers(200, 256, d[::7].shape[0])
+    g.delays = d.astype(np.int32)
+    ev, steps = W.random_events(18, g, 3, [600, 300, 450], rate=0.3)
+    lif = R.LIFParams(threshold=1.0, decay=0.95, reset=0.0, refractory=1, reset_mode=1)
+    ref = O.forward_batched(g, ev, steps, lif)
+    assert int(ref["spikes"].sum()) > 0
+    out = run_gpu(g, ev, steps, lif, R.MODE_SORT, path, force_grid=force)
+    assert_exact(out, ref)
