@@ -307,6 +307,15 @@ int snc_b200_bptt_backward(snc_b200_bptt* h, const float* w, const float* ext, i
                            int32_t smooth, const float* spikes, const uint32_t* spike_bits,
                            const float* v_saved, const float* grad_spikes, float* grad_w,
                            float* grad_ext, void* stream);
+/* Leaky integration along time (the leaky readouts of python/snc/shd_model.py:
+ * 139-140 and python/snc/lm.py:90 as one kernel): x, y [T][n] fp32 device
+ * tensors, y[t] = decay * y[t-1] + x[t] with y[-1] = 0, or with reverse != 0
+ * y[t] = decay * y[t+1] + x[t] from the last step (the gradient); the product
+ * and the sum are rounded separately, as the step loop does.  x and y must not
+ * overlap.  Asynchronous on stream. */
+int snc_b200_leaky_scan(const float* x, float* y, int32_t T, int64_t n, float decay, int32_t reverse,
+                        void* stream);
+
 /* The BPTT forward for callers that must not allocate device memory when
  * they call it (no counterpart in the reference, which allocates inside every
  * GPU call): a stream being captured under a mode that forbids allocation, a

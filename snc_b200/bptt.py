@@ -23,6 +23,7 @@ import sys
 import numpy as np
 import torch
 import torch.nn as nn
+import torch.nn.functional as F
 
 from . import _lib
 from ._lib import check, lib
@@ -174,6 +175,35 @@ class SNN(nn.Module):
         return torch.zeros(B, self.n_out, device=dev).index_add(1, self.out_ch, s.sum(0)[:, self.out_ids])
 
 
+class LeakyScan(torch.autograd.Function):
+    """y[t] = decay * y[t-1] + x[t] along dim 0 of a [T, ...] fp32 CUDA tensor
+    (snc_b200_leaky_scan): the leaky readout loops of shd_model.py:139-140 and
+    lm.py:90 in one kernel, same roundings; the gradient is the reverse scan."""
+
+    @staticmethod
+    def forward(ctx, x, decay):
+        x = x.contiguous().float()
+        y = torch.empty_like(x)
+        T = x.shape[0]
+        check(lib().snc_b200_leaky_scan(_ptr(x), _ptr(y), T, x.numel() // max(1, T), float(decay), 0,
+                                        _stream()), "leaky_scan")
+        ctx.decay = float(decay)
+        return y
+
+    @staticmethod
+    def backward(ctx, g):
+        g = g.contiguous().float()
+        gx = torch.empty_like(g)
+        T = g.shape[0]
+        check(lib().snc_b200_leaky_scan(_ptr(g), _ptr(gx), T, g.numel() // max(1, T), ctx.decay, 1,
+                                        _stream()), "leaky_scan")
+        return gx, None
+
+
+def leaky_scan(x, decay):
+    return LeakyScan.apply(x, decay)
+
+
 class DelayedSNN(nn.Module):
     """Input spikes -> sparse delayed spiking graph -> leaky readout
     (shd_model.py leaky readout: out = ro_decay*out + Linear(s_top),
@@ -206,10 +236,11 @@ class DelayedSNN(nn.Module):
         ext = torch.zeros(T, B, self.N, device=self.w.device)
         ext[:, :, :self.n_in] = spikes_in * self.gain
         s = spiking_core(self.w, ext, self.core(), self.thr, self.decay, self.slope, self.ckpt_every)
-        top = s[:, :, self.ro_ids]
-        out = torch.zeros(B, self.readout.out_features, device=self.w.device)
-        for t in range(T):
-            out = self.ro_decay * out + self.readout(top[t])
+        # out(T-1) of out = ro_decay * out + readout(s_top): the readout of the
+        # leaky-integrated spikes plus the bias summed with the same decay
+        r = leaky_scan(s[:, :, self.ro_ids], self.ro_decay)[T - 1]
+        bias_gain = float(sum(self.ro_decay ** k for k in range(T)))
+        out = F.linear(r, self.readout.weight) + self.readout.bias * bias_gain
         return out / T
 
 
@@ -244,9 +275,5 @@ class SpikingLM(nn.Module):
         ext = self.embed(x).transpose(0, 1)                       # [T, B, H]
         s = spiking_core(self.w_rec, ext, self.core(), self.thr, self.decay, self.slope,
                          self.ckpt_every)
-        r = torch.zeros(B, self.H, device=x.device)
-        rs = []
-        for t in range(T):
-            r = self.ro_decay * r + s[t]
-            rs.append(r)
-        return self.readout(torch.stack(rs, dim=1))
+        r = leaky_scan(s, self.ro_decay)                          # [T, B, H]
+        return self.readout(r.transpose(0, 1))

@@ -372,6 +372,24 @@ static int check_err(snc_b200_bptt* h, cudaStream_t st) {
 
 using namespace sncb;
 
+// Leaky integration along time of a [T][n] tensor: y[t] = decay * y[t-1] +
+// x[t] (reverse: from the last step backwards, y[t] = decay * y[t+1] + x[t]),
+// each product and sum rounded separately like the step-by-step loop of the
+// readouts (shd_model.py:139-140, lm.py:90); the reverse form is its
+// gradient.  One thread per column j, coalesced rows.
+__global__ void k_leaky_scan(const float* __restrict__ x, float* __restrict__ y, int T, long long n,
+                             float decay, int reverse) {
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (long long)gridDim.x * blockDim.x) {
+    float acc = 0.f;
+    for (int k = 0; k < T; ++k) {
+      const long long t = reverse ? T - 1 - k : k;
+      acc = __fadd_rn(__fmul_rn(decay, acc), x[t * n + j]);
+      y[t * n + j] = acc;
+    }
+  }
+}
+
 extern "C" {
 
 int snc_b200_bptt_create(int32_t N, int32_t S, const int32_t* row_ptr, const int32_t* post,
@@ -494,6 +512,20 @@ int snc_b200_bptt_backward(snc_b200_bptt* h, const float* w, const float* ext, i
   SNCB_CUDA(cudaMemsetAsync(grad_w, 0, (size_t)std::max(1, h->S) * sizeof(float), st));
   if ((rc = launch(false, smooth != 0, a, h->sm_count, st))) return rc;
   return check_err(h, st);
+}
+
+int snc_b200_leaky_scan(const float* x, float* y, int32_t T, int64_t n, float decay, int32_t reverse,
+                        void* stream) {
+  if ((T > 0 && n > 0) && (!x || !y)) { set_error("null tensor"); return SNC_B200_EINVAL; }
+  if (T < 0 || n < 0) { set_error("negative size"); return SNC_B200_EINVAL; }
+  if (T == 0 || n == 0) return SNC_B200_OK;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = (int)std::max(1ll, std::min<long long>(((long long)n + 255) / 256, (long long)sms * 16));
+  k_leaky_scan<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(x, y, T, n, decay, reverse ? 1 : 0);
+  SNCB_CUDA(cudaGetLastError());
+  return SNC_B200_OK;
 }
 
 }  // extern "C"

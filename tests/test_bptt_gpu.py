@@ -164,3 +164,51 @@ def test_spiking_lm_gradients():
     assert s.sum() > 0
     rel_close(lm.w_rec.grad.cpu(), wr.grad, 1e-4)
     rel_close(lm.embed.weight.grad.cpu(), emb.grad, 1e-4)
+
+
+def test_leaky_scan_matches_the_step_loop():
+    torch.manual_seed(3)
+    x = torch.randn(37, 5, 29, device=DEV)
+    y = BP.leaky_scan(x, 0.9)
+    r = torch.zeros(5, 29, device=DEV)
+    ref = []
+    for t in range(37):
+        r = 0.9 * r + x[t]
+        ref.append(r)
+    assert torch.equal(y, torch.stack(ref))  # same roundings as the loop
+    xg = x.clone().requires_grad_(True)
+    g = torch.randn_like(x)
+    (BP.leaky_scan(xg, 0.9) * g).sum().backward()
+    xr = x.clone().requires_grad_(True)
+    r = torch.zeros(5, 29, device=DEV)
+    out = []
+    for t in range(37):
+        r = 0.9 * r + xr[t]
+        out.append(r)
+    (torch.stack(out) * g).sum().backward()
+    rel_close(xg.grad.cpu(), xr.grad.cpu(), 1e-6)
+
+
+def test_delayed_snn_readout_and_gradients():
+    d = W.random_graph(8, n_in=20, n_hid=60, n_out=6, max_delay=4)
+    pre = d.pre_ids()
+    ro_ids = np.nonzero(np.asarray(d.role) == 2)[0]
+    net = BP.DelayedSNN(d.num_neurons, pre, d.post_ids, d.delays, 20, ro_ids, 3, thr=1.0,
+                        decay=0.9, surrogate_scale=25.0, ckpt_every=0, seed=2).to(DEV)
+    T, B = 24, 7
+    x = (torch.rand(T, B, 20, generator=torch.Generator().manual_seed(4)) < 0.3).float()
+    F = torch.nn.functional
+    y = torch.as_tensor(np.random.default_rng(1).integers(0, 3, B))
+    F.cross_entropy(net(x.to(DEV)), y.to(DEV)).backward()
+    wt = net.w.detach().cpu().clone().requires_grad_(True)
+    wro = net.readout.weight.detach().cpu().clone().requires_grad_(True)
+    bro = net.readout.bias.detach().cpu().clone().requires_grad_(True)
+    ext = torch.zeros(T, B, d.num_neurons)
+    ext[:, :, :20] = x
+    s = BR.core_forward(wt, ext, torch.as_tensor(pre).long(), torch.as_tensor(d.post_ids).long(),
+                        torch.as_tensor(d.delays).long(), 1.0, 0.9, 25.0)
+    F.cross_entropy(BR.leaky_readout(s, wro, bro, torch.as_tensor(ro_ids).long(), 0.9), y).backward()
+    assert s.sum() > 0
+    rel_close(net.w.grad.cpu(), wt.grad, 1e-4)
+    rel_close(net.readout.weight.grad.cpu(), wro.grad, 1e-4)
+    rel_close(net.readout.bias.grad.cpu(), bro.grad, 1e-4)
