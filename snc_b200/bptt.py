@@ -238,7 +238,7 @@ class DelayedSNN(nn.Module):
         s = spiking_core(self.w, ext, self.core(), self.thr, self.decay, self.slope, self.ckpt_every)
         # out(T-1) of out = ro_decay * out + readout(s_top): the readout of the
         # leaky-integrated spikes plus the bias summed with the same decay
-        r = leaky_scan(s[:, :, self.ro_ids], self.ro_decay)[T - 1]
+        r = leaky_scan(s.index_select(2, self.ro_ids), self.ro_decay)[T - 1]
         bias_gain = float(sum(self.ro_decay ** k for k in range(T)))
         out = F.linear(r, self.readout.weight) + self.readout.bias * bias_gain
         return out / T

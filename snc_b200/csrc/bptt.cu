@@ -69,6 +69,10 @@ constexpr int kBpThreads = 256;
 // One step of the forward for neuron j.  v holds the neuron's state before
 // the step (per lane, batch elements lane + 32k) and is updated; vp receives
 // the pre-reset potential; s the spike.
+// Edges whose spike words / future gradients one lane keeps in flight.
+template <int KB>
+constexpr int kEdgeBatch = KB >= 8 ? 4 : 8;
+
 template <int KB, bool SMOOTH>
 __device__ __forceinline__ void fwd_neuron(const BpArgs& a, int t, int j, float (&v)[KB],
                                            float (&vp)[KB], float (&s)[KB]) {
@@ -86,18 +90,39 @@ __device__ __forceinline__ void fwd_neuron(const BpArgs& a, int t, int j, float 
       my_d = a.in_d[eb + lane];
       my_w = a.w[a.in_eidx[eb + lane]];
     }
+    if (!SMOOTH) {
+      // the spike words of kEdgeBatch edges are loaded together, then added
+      // in edge order (the order of the sum is unchanged)
+      for (int q0 = 0; q0 < n; q0 += kEdgeBatch<KB>) {
+        uint32_t wv[kEdgeBatch<KB>][KB];
+        float wwv[kEdgeBatch<KB>];
+#pragma unroll
+        for (int u = 0; u < kEdgeBatch<KB>; ++u) {
+          const int q = q0 + u;
+          const int pre = __shfl_sync(0xffffffffu, my_pre, q & 31);
+          const int d = __shfl_sync(0xffffffffu, my_d, q & 31);
+          wwv[u] = __shfl_sync(0xffffffffu, my_w, q & 31);
+          const int ts = t - d;
+          const bool ok = q < n && ts >= 0;
+          const uint32_t* wp = a.bits + ((size_t)(ok ? ts : 0) * a.N + pre) * KB;
+#pragma unroll
+          for (int k = 0; k < KB; ++k) wv[u][k] = ok ? wp[k] : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < kEdgeBatch<KB>; ++u)
+#pragma unroll
+          for (int k = 0; k < KB; ++k)
+            if ((wv[u][k] >> lane) & 1u) acc[k] = __fadd_rn(acc[k], wwv[u]);
+      }
+      continue;
+    }
     for (int q = 0; q < n; ++q) {
       const int pre = __shfl_sync(0xffffffffu, my_pre, q);
       const int d = __shfl_sync(0xffffffffu, my_d, q);
       const float ww = __shfl_sync(0xffffffffu, my_w, q);
       const int ts = t - d;
       if (ts < 0) continue;
-      if (!SMOOTH) {
-        const uint32_t* wp = a.bits + ((size_t)ts * a.N + pre) * KB;
-#pragma unroll
-        for (int k = 0; k < KB; ++k)
-          if ((wp[k] >> lane) & 1u) acc[k] = __fadd_rn(acc[k], ww);
-      } else {
+      {
         const float* sp = a.spikes + ((size_t)ts * a.N + pre) * a.B;
 #pragma unroll
         for (int k = 0; k < KB; ++k) {
@@ -185,18 +210,35 @@ __device__ __forceinline__ void bwd_neuron(const BpArgs& a, int t, int i, const 
       my_d = a.out_d[eb + lane];
       my_w = a.w[eb + lane];
     }
-    for (int q = 0; q < n; ++q) {
-      const int post = __shfl_sync(0xffffffffu, my_post, q);
-      const int d = __shfl_sync(0xffffffffu, my_d, q);
-      const float ww = __shfl_sync(0xffffffffu, my_w, q);
-      const int tt = t + d;
-      if (tt >= a.T) continue;
-      const float* gp = a.gcur + ((size_t)(tt % a.R) * N + post) * B;
+    // the future gradients of kEdgeBatch edges are loaded together, then
+    // accumulated in edge order
+    for (int q0 = 0; q0 < n; q0 += kEdgeBatch<KB>) {
+      float gv[kEdgeBatch<KB>][KB];
+      float wwv[kEdgeBatch<KB>];
+      bool okv[kEdgeBatch<KB>];
 #pragma unroll
-      for (int k = 0; k < KB; ++k) {
-        const int b = 32 * k + lane;
-        if (b < B) gs[k] = __fadd_rn(gs[k], __fmul_rn(ww, gp[b]));
+      for (int u = 0; u < kEdgeBatch<KB>; ++u) {
+        const int q = q0 + u;
+        const int post = __shfl_sync(0xffffffffu, my_post, q & 31);
+        const int d = __shfl_sync(0xffffffffu, my_d, q & 31);
+        wwv[u] = __shfl_sync(0xffffffffu, my_w, q & 31);
+        const int tt = t + d;
+        okv[u] = q < n && tt < a.T;
+        const float* gp = a.gcur + ((size_t)(okv[u] ? tt % a.R : 0) * N + post) * B;
+#pragma unroll
+        for (int k = 0; k < KB; ++k) {
+          const int b = 32 * k + lane;
+          gv[u][k] = okv[u] && b < B ? gp[b] : 0.f;
+        }
       }
+#pragma unroll
+      for (int u = 0; u < kEdgeBatch<KB>; ++u)
+        if (okv[u])
+#pragma unroll
+          for (int k = 0; k < KB; ++k) {
+            const int b = 32 * k + lane;
+            if (b < B) gs[k] = __fadd_rn(gs[k], __fmul_rn(wwv[u], gv[u][k]));
+          }
     }
   }
   float* gc = a.gcur + ((size_t)(t % a.R) * N + i) * B;
