@@ -160,7 +160,7 @@ __device__ __forceinline__ void apply_one(float* ring, int ring_stride, int col0
 // always links in order: its post blocks own hub columns whose per-step
 // event count can be large.
 constexpr int kSerialLinkMax = 192;
-constexpr int kRegSort = 8;
+constexpr int kRegSort = 16;
 constexpr int kFirstFlag = 1 << 30;  // marks a group's first event of its column in st_col
 
 // Ordered apply of one chunk of staged events.  Staging index q is the
@@ -422,7 +422,12 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
         int base = 0;
         for (int k0 = 0; k0 < nf; k0 += nthr) {
           const int k = k0 + tid;
-          const int len = k < nf ? a.row_ptr[fired[k] + 1] - a.row_ptr[fired[k]] : 0;
+          int len = 0;
+          if (k < nf) {
+            const int rs = a.row_ptr[fired[k]];
+            len = a.row_ptr[fired[k] + 1] - rs;
+            fired[k] = rs;  // row start from here on (the list is not used again this step)
+          }
           int tot;
           const int ex = block_exclusive_scan(len, scratch, &tot);
           if (k < nf) pref[k] = base + ex;
@@ -435,7 +440,7 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
           for (int qq = tid; qq < ce; qq += nthr) {
             const int e = e0 + qq;
             const int k = upper_index(pref, nf, e);
-            const uint2 ed = a.edges[a.row_ptr[fired[k]] + (e - pref[k])];
+            const uint2 ed = a.edges[fired[k] + (e - pref[k])];
             st_slot[qq] = ring_slot(s0, edge_delay(ed), R);
             st_w[qq] = edge_w(ed);
             st_col[qq] = edge_col(ed);
