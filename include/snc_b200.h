@@ -251,6 +251,10 @@ typedef struct snc_b200_eprop snc_b200_eprop; /* cudatrain::CudaTrainSession */
 int snc_b200_eprop_create(const snc_b200_graph* g, const snc_lif* lif, const snc_eprop_cfg* cfg,
                           int32_t max_batch, const float* weights, const float* feedback,
                           snc_b200_eprop** out);
+/* Which forward a session runs: SNC_B200_PATH_PLAIN when one sample's state
+ * fits one CTA (the sample-per-CTA kernel), SNC_B200_PATH_PERSISTENT when it
+ * does not (the all-SM kernel on a destination-grouped copy of the weights). */
+int snc_b200_eprop_path(const snc_b200_eprop* s);
 int snc_b200_eprop_release(snc_b200_eprop* s);                    /* cudatrain::destroy */
 int snc_b200_eprop_set_weights(snc_b200_eprop* s, const float* w); /* [S] */
 int snc_b200_eprop_get_weights(snc_b200_eprop* s, float* w);       /* [S] */

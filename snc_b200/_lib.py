@@ -74,6 +74,7 @@ SIGNATURES = {
     "snc_b200_autotune": (C.c_int, [P, P, P, P, P, P]),
     "snc_b200_eprop_create": (C.c_int, [P, P, P, I32, P, P, P]),
     "snc_b200_eprop_release": (C.c_int, [P]),
+    "snc_b200_eprop_path": (C.c_int, [P]),
     "snc_b200_eprop_set_weights": (C.c_int, [P, P]),
     "snc_b200_eprop_get_weights": (C.c_int, [P, P]),
     "snc_b200_eprop_batch": (C.c_int, [P, P, C.c_size_t, I32, P, P, C.c_int, P, P]),

@@ -43,6 +43,13 @@ struct snc_b200_eprop {
   // deferred eligibility: the forward records psi per ring column and step
   // and the spike raster; k_elig_deferred then builds E from them
   sncb::DevBuf psi_hist, raster;
+  // grid mode: one sample's state does not fit one CTA's shared memory, so
+  // the forward runs on the all-SM kernel, which reads destination-grouped
+  // edges: a grouped copy of the trainer's weights, kept in step with them
+  bool grid = false;
+  int* gperm = nullptr;           // [S] CSR edge -> its grouped position
+  uint2* gedges = nullptr;        // [S+2]
+  sncb::Run* run = nullptr;
 };
 
 namespace sncb {
@@ -113,6 +120,19 @@ __global__ void k_get_weights(int S, const uint2* edges, float* w) {
 
 static inline int grid_of(long long n, int b = 256) { return (int)std::max(1ll, (n + b - 1) / b); }
 
+// The grouped copy of the trainer's weights follows the CSR edges.
+__global__ void k_sync_gedges(int S, const uint2* edges, const int* gperm, uint2* gedges) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < S) gedges[gperm[e]].y = edges[e].y;
+}
+
+static int sync_gedges(snc_b200_eprop* s, cudaStream_t st) {
+  if (!s->grid || s->g->S == 0) return SNC_B200_OK;
+  k_sync_gedges<<<grid_of(s->g->S), 256, 0, st>>>(s->g->S, s->edges, s->gperm, s->gedges);
+  SNCB_CUDA(cudaGetLastError());
+  return SNC_B200_OK;
+}
+
 // Most bytes the psi history of one minibatch may take; beyond it the
 // eligibility is accumulated inside the forward instead.
 constexpr size_t kPsiHistMax = size_t(2) << 30;
@@ -180,6 +200,20 @@ static void free_session(snc_b200_eprop* s) {
   if (s->ev1) cudaEventDestroy(s->ev1);
   s->psi_hist.release();
   s->raster.release();
+  if (s->run) {
+    // the run borrows the session's outputs and control words
+    s->run->counts = nullptr;
+    s->run->spikes = nullptr;
+    s->run->events = nullptr;
+    s->run->err = nullptr;
+    s->run->ctl = nullptr;
+    s->run->raster = nullptr;
+    free_run(s->run);
+    delete s->run;
+    s->run = nullptr;
+  }
+  dev_free(s->gperm);
+  dev_free(s->gedges);
 }
 
 static int create_session(snc_b200_eprop* s, const Graph* g, const snc_lif* lif,
@@ -219,6 +253,45 @@ static int create_session(snc_b200_eprop* s, const Graph* g, const snc_lif* lif,
   SNCB_CUDA(cudaMemset(s->fires, 0, (size_t)std::max(1, N) * sizeof(unsigned long long)));
   SNCB_CUDA(cudaEventCreate(&s->ev0));
   SNCB_CUDA(cudaEventCreate(&s->ev1));
+  // grid mode when a sample's state and eligibility inputs do not fit one CTA
+  {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const int mode = cfg->mode == SNC_B200_MODE_SORT ? SNC_B200_MODE_SORT : SNC_B200_MODE_ATOMIC;
+    s->grid = tier_s_smem_bytes(g, mode, true) > optin;
+  }
+  if (s->grid) {
+    // the stable regroup of every row by destination block, as the graph's
+    // grouped edges were built
+    std::vector<int> post((size_t)std::max(1, S));
+    if (S) SNCB_CUDA(cudaMemcpy(post.data(), g->post, (size_t)S * 4, cudaMemcpyDeviceToHost));
+    std::vector<int> perm((size_t)std::max(1, S)), idx;
+    std::vector<uint2> ge((size_t)S + 2, make_uint2(0, 0));
+    for (int i = 0; i < N; ++i) {
+      const int rs = g->row_ptr_h[i], re = g->row_ptr_h[i + 1];
+      idx.resize(re - rs);
+      for (int q = 0; q < re - rs; ++q) idx[q] = rs + q;
+      std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return post[x] / g->BS < post[y] / g->BS; });
+      for (int q = 0; q < re - rs; ++q) {
+        perm[idx[q]] = rs + q;
+        ge[rs + q] = edges[idx[q]];
+      }
+    }
+    if ((rc = dev_upload(&s->gperm, perm.data(), perm.size()))) return rc;
+    if ((rc = dev_upload(&s->gedges, ge.data(), ge.size()))) return rc;
+    s->run = new Run();
+    Run& r = *s->run;
+    r.g = g;
+    r.W = (N + 31) / 32;
+    r.counts = s->counts;
+    r.spikes = s->spikes;
+    r.events = s->events;
+    r.err = s->err;
+    r.ctl = s->ctl;
+    SNCB_CUDA(cudaEventCreate(&r.ev0));
+    SNCB_CUDA(cudaEventCreate(&r.ev1));
+  }
   return SNC_B200_OK;
 }
 
@@ -272,6 +345,11 @@ static int run_batch(snc_b200_eprop* s, const snc_input_event* ev, size_t n_ev, 
   const int W = (N + 31) / 32;
   const size_t psi_bytes = (size_t)B * std::max(1, g->ncols) * std::max(1, in.Tmax) * sizeof(float);
   const bool deferred = train && psi_bytes <= kPsiHistMax;
+  if (train && s->grid && !deferred) {
+    free_inputs(&in);
+    set_error("e-prop: the minibatch's psi history exceeds its budget on the grid path; use fewer samples or steps");
+    return SNC_B200_EUNSUPPORTED;
+  }
   if (deferred) {
     if ((rc = s->psi_hist.reserve(psi_bytes))) { free_inputs(&in); return rc; }
     if ((rc = s->raster.reserve((size_t)std::max(1ll, in.raster_words) * sizeof(uint32_t)))) {
@@ -285,7 +363,23 @@ static int run_batch(snc_b200_eprop* s, const snc_input_event* ev, size_t n_ev, 
     chk(cudaMemcpyAsync(s->steps, steps, (size_t)B * 4, cudaMemcpyHostToDevice, st), "steps");
   }
   chk(cudaEventRecord(s->ev0, st), "event");
-  if (ok) {
+  if (ok && s->grid) {
+    // the all-SM kernel with the trainer's weights, recording psi and the
+    // raster for the deferred eligibility
+    Run& r = *s->run;
+    r.in = &in;
+    r.flags = SNC_B200_RUN_FORCE_GRID | (deferred ? SNC_B200_RUN_RASTER : 0);
+    r.raster = deferred ? static_cast<uint32_t*>(s->raster.p) : nullptr;
+    r.edges_w = s->edges;
+    r.gedges_w = s->gedges;
+    r.fires = train ? s->fires : nullptr;
+    r.psi_hist = deferred ? static_cast<float*>(s->psi_hist.p) : nullptr;
+    r.psi_T = std::max(1, in.Tmax);
+    r.gamma = s->cfg.surrogate_scale;
+    const int mode = s->cfg.mode == SNC_B200_MODE_SORT ? SNC_B200_MODE_SORT : SNC_B200_MODE_ATOMIC;
+    rc = launch_run(&r, &s->lif, mode, SNC_B200_PATH_PERSISTENT, nullptr);
+    ok = rc == SNC_B200_OK;
+  } else if (ok) {
     EpropLaunch e;
     e.g = g;
     e.in = &in;
@@ -308,7 +402,9 @@ static int run_batch(snc_b200_eprop* s, const snc_input_event* ev, size_t n_ev, 
     e.ctl = s->ctl;
     rc = launch_eprop_forward(e, st);
     ok = rc == SNC_B200_OK;
-    if (ok && deferred) {
+  }
+  if (ok) {
+    if (deferred) {
       int dev = 0, sms = 148;
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -335,6 +431,10 @@ static int run_batch(snc_b200_eprop* s, const snc_input_event* ev, size_t n_ev, 
       k_apply<<<grid_of(S), 256, 0, st>>>(S, N, B, uniform ? 1 : 0, s->cfg.lr, lr_over_T,
                                           s->cfg.w_max, g->post, s->steps, s->L, s->elig, s->edges);
     chk(cudaGetLastError(), "e-prop update kernels");
+    if (train == 1 && ok) {
+      const int r2 = sync_gedges(s, st);
+      if (r2) { rc = r2; ok = false; }
+    }
   }
   chk(cudaEventRecord(s->ev1, st), "event");
   chk(cudaEventSynchronize(s->ev1), "synchronize");
@@ -393,6 +493,11 @@ int snc_b200_eprop_create(const snc_b200_graph* g, const snc_lif* lif, const snc
   return SNC_B200_OK;
 }
 
+int snc_b200_eprop_path(const snc_b200_eprop* s) {
+  if (!s) { set_error("null session"); return SNC_B200_EINVAL; }
+  return s->grid ? SNC_B200_PATH_PERSISTENT : SNC_B200_PATH_PLAIN;
+}
+
 int snc_b200_eprop_release(snc_b200_eprop* s) {
   if (!s) return SNC_B200_OK;
   free_session(s);
@@ -406,6 +511,8 @@ int snc_b200_eprop_set_weights(snc_b200_eprop* s, const float* w) {
   int rc = dev_upload(&d, w, (size_t)std::max(1, s->g->S));
   if (rc) return rc;
   k_set_weights<<<grid_of(s->g->S), 256>>>(s->g->S, d, s->edges);
+  rc = sync_gedges(s, nullptr);
+  if (rc) { dev_free(d); return rc; }
   cudaError_t e = cudaDeviceSynchronize();
   dev_free(d);
   if (e != cudaSuccess) return cuda_fail(e, "set_weights");
@@ -443,6 +550,8 @@ int snc_b200_eprop_apply(snc_b200_eprop* s, const float* grad, int32_t total_bat
   k_apply_grad<<<grid_of(s->g->S), 256>>>(s->g->S, s->cfg.lr, s->cfg.w_max, total_batch, grad,
                                           s->edges);
   SNCB_CUDA(cudaGetLastError());
+  int rc = sync_gedges(s, nullptr);
+  if (rc) return rc;
   SNCB_CUDA(cudaDeviceSynchronize());
   return SNC_B200_OK;
 }

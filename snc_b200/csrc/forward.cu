@@ -607,7 +607,16 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, unsigne
       }
       const float e = ext[jj];
       ext[jj] = 0.f;
-      f = lif_step(a.lif, vv, rr, e, rin);
+      float vpre;
+      f = lif_step(a.lif, vv, rr, e, rin, &vpre);
+      if (a.psi_hist && c >= 0) {
+        // e-prop (cuda_trainer.cu:151-152): the triangular surrogate of this
+        // column and step, for the deferred eligibility
+        const float thr = a.lif.thr;
+        const float dd = __fdiv_rn(fabsf(__fsub_rn(vpre, thr)), thr > 0.f ? thr : 1.f);
+        a.psi_hist[((size_t)sample * nc + c) * a.psi_T + t] =
+            dd < 1.f ? __fmul_rn(a.gamma, __fsub_rn(1.f, dd)) : 0.f;
+      }
       if (PERSIST) {
         sm.v[k * BS + jj] = vv;
         sm.refr[k * BS + jj] = rr;
@@ -619,6 +628,7 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, unsigne
         my_events += PERSIST ? sm.rp[jj + 1] - sm.rp[jj] : a.row_ptr[j + 1] - a.row_ptr[j];
         const int oc = PERSIST ? sm.och[jj] : a.out_ch[j];
         if (oc >= 0) atomicAdd(&a.counts[(size_t)sample * a.noc + oc], 1);
+        if (a.fires) atomicAdd(&a.fires[j], 1ull);
       }
     }
     int tot;
@@ -1031,6 +1041,12 @@ static FwdArgs make_args(Run* r, const snc_lif* lif) {
   a.fired_cnt = r->fired_cnt; a.inbox = r->inbox; a.inbox_cnt = r->inbox_cnt;
   a.err = r->err; a.ctl = r->ctl;
   a.lif = LifP{lif->threshold, lif->decay, lif->reset, lif->refractory, lif->reset_mode};
+  if (r->edges_w) a.edges = r->edges_w;
+  if (r->gedges_w) a.gedges = r->gedges_w;
+  a.psi_hist = r->psi_hist;
+  a.psi_T = r->psi_T;
+  a.fires = r->fires;
+  a.gamma = r->gamma;
   return a;
 }
 

@@ -177,6 +177,15 @@ struct Run {
   cudaStream_t own_stream = nullptr;  // stands in for the legacy default stream
   bool graph_refused = false;         // stream capture failed once; launch directly
   bool used_graph = false;            // the last launch went through the graph
+  // e-prop through the grid path (all null for a forward): the trainer's
+  // weights in CSR and destination-grouped order, and what the deferred
+  // eligibility reads -- psi per ring column and step, per-neuron fire counts
+  const uint2* edges_w = nullptr;
+  const uint2* gedges_w = nullptr;
+  float* psi_hist = nullptr;  // [B][ncols][psi_T]
+  int psi_T = 0;
+  unsigned long long* fires = nullptr;
+  float gamma = 0.f;
 };
 
 // One e-prop minibatch forward (tier S kernel with eligibility).

@@ -90,6 +90,11 @@ class CudaTrainSession:
             raise ValueError("weights must have one entry per synapse")
         check(lib().snc_b200_eprop_set_weights(self.h, ptr(w)), "eprop_set_weights")
 
+    def uses_grid(self) -> bool:
+        """True when the forward runs on the all-SM kernel (one sample's state
+        does not fit one CTA's shared memory)."""
+        return lib().snc_b200_eprop_path(self.h) == _lib.PATH_PERSISTENT
+
     def get_weights(self) -> np.ndarray:
         w = np.zeros(self.g.num_synapses, np.float32)
         check(lib().snc_b200_eprop_get_weights(self.h, ptr(w)), "eprop_get_weights")

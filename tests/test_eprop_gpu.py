@@ -129,3 +129,45 @@ def test_gradient_shards_and_apply():
     s2 = E.CudaTrainSession(g, cfg, batch=8, weights=w0, feedback=fb)
     PAR.DataParallelEprop(s2, g.num_synapses).step(ev, st, labels)
     np.testing.assert_allclose(s2.get_weights(), ref["w"], rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize("mode", [R.MODE_SORT, R.MODE_ATOMIC])
+def test_eprop_on_the_all_sm_path(mode):
+    """A sample's state that does not fit one CTA (delays up to 250: a
+    251-slot ring) trains on the all-SM kernel: the same eligibility (SORT:
+    bit for bit) and update as the restatement, and a second minibatch after
+    the update sees the new weights."""
+    g = W.random_graph(31, n_hid=300, max_delay=6)
+    rng = np.random.default_rng(31)
+    d = g.delays.copy()
+    d[::3] = rng.integers(100, 251, d[::3].shape[0])
+    g.delays = d.astype(np.int32)
+    ev, st = W.random_events(32, g, 3, [40, 25, 33])
+    w0 = rng.normal(0, 0.5, g.num_synapses).astype(np.float32)
+    n_int = int((g.role == INTERNAL).sum())
+    fb = rng.normal(0, 1.0, (n_int, g.num_output_channels)).astype(np.float32)
+    labels = rng.integers(0, g.num_output_channels, 3).astype(np.int32)
+    lif = R.LIFParams(threshold=1.0, decay=0.9, reset=0.0, refractory=1)
+    cfg = E.TrainConfig(lif=lif, lr=0.5, w_max=4.0, surrogate_scale=0.3, trace_decay=0.95, mode=mode)
+    s = E.CudaTrainSession(g, cfg, batch=4, weights=w0, feedback=fb)
+    assert s.uses_grid()
+    fires = np.zeros(g.num_neurons, np.int64)
+    ref = O.eprop_batch(g, w0, ev, st, lif, trace_decay=0.95, gamma=0.3, lr=0.5, w_max=4.0,
+                        train_hidden=True, bmat=fb, labels=labels, want_elig=True, fires=fires)
+    out = s.run_batch(ev, st, labels, train=True)
+    assert ref["spikes"] > 0
+    if mode == R.MODE_SORT:
+        np.testing.assert_array_equal(out["counts"], ref["counts"])
+        assert out["spikes"] == ref["spikes"] and out["events"] == ref["events"]
+        np.testing.assert_array_equal(s.eligibility(3).view(np.uint32), ref["elig"].view(np.uint32))
+        np.testing.assert_allclose(s.get_weights(), ref["w"], rtol=1e-5, atol=1e-7)
+        np.testing.assert_array_equal(s.collect_stats()[1], fires)
+        # second minibatch on the updated weights
+        ev2, st2 = W.random_events(33, g, 2, [30, 30])
+        lab2 = labels[:2]
+        ref2 = O.eprop_batch(g, s.get_weights(), ev2, st2, lif, trace_decay=0.95, gamma=0.3, lr=0.5,
+                             w_max=4.0, train_hidden=True, bmat=fb, labels=lab2, train=False)
+        out2 = s.run_batch(ev2, st2, train=False)
+        np.testing.assert_array_equal(out2["counts"], ref2["counts"])
+    else:
+        assert abs(out["spikes"] - ref["spikes"]) <= 0.001 * ref["spikes"] + 2
