@@ -571,7 +571,8 @@ __device__ void load_ext(const FwdArgs& a, float* ext, int sample, long long gst
 // acc: per-slot spike / event totals in shared memory ([0, kMaxWave) spikes,
 // [kMaxWave, 2 kMaxWave) events) that the caller adds to the sample's totals
 // once per wave; null: added to the global totals every step.
-template <int MODE, bool PERSIST, bool RSM>
+// EPR: record e-prop's psi and fire counts (the all-SM e-prop forward only).
+template <int MODE, bool PERSIST, bool RSM, bool EPR = false>
 __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, unsigned long long* acc,
                         int k, int sample, long long gstep, int t, int b, int cb0, bool ext_ready) {
   const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5;
@@ -608,8 +609,8 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, unsigne
       const float e = ext[jj];
       ext[jj] = 0.f;
       float vpre;
-      f = lif_step(a.lif, vv, rr, e, rin, &vpre);
-      if (a.psi_hist && c >= 0) {
+      f = lif_step(a.lif, vv, rr, e, rin, EPR ? &vpre : nullptr);
+      if (EPR && c >= 0) {
         // e-prop (cuda_trainer.cu:151-152): the triangular surrogate of this
         // column and step, for the deferred eligibility
         const float thr = a.lif.thr;
@@ -628,7 +629,7 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, unsigne
         my_events += PERSIST ? sm.rp[jj + 1] - sm.rp[jj] : a.row_ptr[j + 1] - a.row_ptr[j];
         const int oc = PERSIST ? sm.och[jj] : a.out_ch[j];
         if (oc >= 0) atomicAdd(&a.counts[(size_t)sample * a.noc + oc], 1);
-        if (a.fires) atomicAdd(&a.fires[j], 1ull);
+        if (EPR && a.fires) atomicAdd(&a.fires[j], 1ull);
       }
     }
     int tot;
@@ -882,7 +883,7 @@ __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, 
   }
 }
 
-template <int MODE, bool RSM>
+template <int MODE, bool RSM, bool EPR>
 __global__ void __launch_bounds__(kGThreadsMax, 1) k_tier_g(FwdArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int scratch[40];
@@ -942,7 +943,7 @@ __global__ void __launch_bounds__(kGThreadsMax, 1) k_tier_g(FwdArgs a) {
     for (int t = 0; t < Tw; ++t) {
       for (int k = 0; k < nk; ++k)
         if (t < s_T[k])
-          phase_a<MODE, true, RSM>(a, sm, scratch, s_acc, k, s_samp[k], s_gb[k] + t, t, b, cb0,
+          phase_a<MODE, true, RSM, EPR>(a, sm, scratch, s_acc, k, s_samp[k], s_gb[k] + t, t, b, cb0,
                                    t > 0);
       // arrive, fetch the next step's drive while the other blocks catch up,
       // then wait
@@ -1166,13 +1167,13 @@ static int tier_g_threads(const Graph* g) {
   return std::max(kGThreads, std::min(kGThreadsMax, (g->BS + 31) / 32 * 32));
 }
 
-template <int MODE, bool RSM>
+template <int MODE, bool RSM, bool EPR>
 static int launch_tier_g(Run* r, const FwdArgs& a, size_t smem, cudaStream_t st) {
   const Graph* g = r->g;
   const int nthr = tier_g_threads(g);
-  SNCB_CUDA(cudaFuncSetAttribute(k_tier_g<MODE, RSM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  SNCB_CUDA(cudaFuncSetAttribute(k_tier_g<MODE, RSM, EPR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  SNCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tier_g<MODE, RSM>, nthr, smem));
+  SNCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tier_g<MODE, RSM, EPR>, nthr, smem));
   if (per_sm * g->sm_count < g->P) {
     set_error("grid tier: blocks cannot be co-resident");
     return SNC_B200_EUNSUPPORTED;
@@ -1187,7 +1188,7 @@ static int launch_tier_g(Run* r, const FwdArgs& a, size_t smem, cudaStream_t st)
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  SNCB_CUDA(cudaLaunchKernelEx(&cfg, k_tier_g<MODE, RSM>, a));
+  SNCB_CUDA(cudaLaunchKernelEx(&cfg, k_tier_g<MODE, RSM, EPR>, a));
   return SNC_B200_OK;
 }
 
@@ -1232,13 +1233,18 @@ static int launch_body(Run* r, const FwdArgs& a, int mode, int path, cudaStream_
   }
   if (path == SNC_B200_PATH_PERSISTENT) {
     const size_t smem = r->gplan_smem;
-    if (mode == MODE_ATOMIC) return launch_tier_g<MODE_ATOMIC, false>(r, a, smem, st);
-    if (r->gplan_rsm) {
-      if (mode == MODE_SORT) return launch_tier_g<MODE_SORT, true>(r, a, smem, st);
-      return launch_tier_g<MODE_BUCKET, true>(r, a, smem, st);
+    if (r->psi_hist || r->fires) {  // e-prop: ATOMIC or SORT delivery
+      if (mode == MODE_ATOMIC) return launch_tier_g<MODE_ATOMIC, false, true>(r, a, smem, st);
+      if (r->gplan_rsm) return launch_tier_g<MODE_SORT, true, true>(r, a, smem, st);
+      return launch_tier_g<MODE_SORT, false, true>(r, a, smem, st);
     }
-    if (mode == MODE_SORT) return launch_tier_g<MODE_SORT, false>(r, a, smem, st);
-    return launch_tier_g<MODE_BUCKET, false>(r, a, smem, st);
+    if (mode == MODE_ATOMIC) return launch_tier_g<MODE_ATOMIC, false, false>(r, a, smem, st);
+    if (r->gplan_rsm) {
+      if (mode == MODE_SORT) return launch_tier_g<MODE_SORT, true, false>(r, a, smem, st);
+      return launch_tier_g<MODE_BUCKET, true, false>(r, a, smem, st);
+    }
+    if (mode == MODE_SORT) return launch_tier_g<MODE_SORT, false, false>(r, a, smem, st);
+    return launch_tier_g<MODE_BUCKET, false, false>(r, a, smem, st);
   }
   if (mode == MODE_SORT) return launch_plain<MODE_SORT>(r, a, st);
   if (mode == MODE_BUCKET) return launch_plain<MODE_BUCKET>(r, a, st);
