@@ -25,6 +25,7 @@ from its sources into oracle/_ref, snc::forward with the OpenMP backend, all
 host threads) on the same workload; rank 0 only.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py --leg bptt|bptt-custom|configs   # one extra leg alone (profiling)
 """
 from __future__ import annotations
 
@@ -56,6 +57,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--mode", default="auto", choices=["auto", "atomic", "bucket", "sort"])
     p.add_argument("--no-extra", action="store_true", help="skip the plain / sort / cpu legs")
+    p.add_argument("--leg", choices=["bptt", "bptt-custom", "configs"],
+                   help="run only this extra leg on one GPU and print its JSON (for profiling)")
     return p.parse_args()
 
 
@@ -323,14 +326,16 @@ def config_legs(reps=3):
     return out
 
 
-def bptt_leg(steps=3, warmup=2, lm=True):
+def bptt_leg(steps=3, warmup=2, lm=True, with_reference=True):
     """BPTT step (forward + backward) of the custom kernels against the
     PyTorch-autograd bridge (oracle/bptt_ref.py, the reference bridge's model
     with per-synapse delays) on the same GPU.
       mnist-like: 784 Poisson -> 512 -> 512 LIF (local sparse, delays 1-4)
                   -> 10 leaky readout, T=100, B=128, checkpoint every 10.
       char-LM:    4096 recurrent LIF, fan-in 64, delays 1-8, 96-symbol
-                  Zipf tokens, B=64, T=256, checkpoint every 16."""
+                  Zipf tokens, B=64, T=256, checkpoint every 16.
+    with_reference=False times the custom steps alone (no bridge, no
+    gradient comparison)."""
     import torch
     import torch.nn.functional as F
 
@@ -369,10 +374,11 @@ def bptt_leg(steps=3, warmup=2, lm=True):
 
     del order
     ms_c = _time_cuda(custom, steps, warmup)
-    ms_r = _time_cuda(reference, steps, warmup)
-    rel = float((model.w.grad - w_ref.grad).abs().max() / w_ref.grad.abs().max().clamp_min(1e-30))
-    out["mnist_like"] = {"custom_ms": ms_c, "autograd_ms": ms_r, "speedup": ms_r / ms_c,
-                         "grad_rel_err": rel, "T": 100, "B": 128, "synapses": int(len(c4["pre"]))}
+    out["mnist_like"] = {"custom_ms": ms_c, "T": 100, "B": 128, "synapses": int(len(c4["pre"]))}
+    if with_reference:
+        ms_r = _time_cuda(reference, steps, warmup)
+        rel = float((model.w.grad - w_ref.grad).abs().max() / w_ref.grad.abs().max().clamp_min(1e-30))
+        out["mnist_like"].update({"autograd_ms": ms_r, "speedup": ms_r / ms_c, "grad_rel_err": rel})
     if lm:
         c5 = W.char_lm()
         torch.manual_seed(0)
@@ -406,11 +412,12 @@ def bptt_leg(steps=3, warmup=2, lm=True):
             F.cross_entropy(lg.reshape(-1, c5["vocab"]), yt.reshape(-1)).backward()
 
         ms_c5 = _time_cuda(lm_custom, 2, 1)
-        ms_r5 = _time_cuda(lm_reference, 1, 1)
-        rel5 = float((net.w_rec.grad - wr.grad).abs().max() / wr.grad.abs().max().clamp_min(1e-30))
-        out["char_lm"] = {"custom_ms": ms_c5, "autograd_ms": ms_r5, "speedup": ms_r5 / ms_c5,
-                          "grad_rel_err": rel5, "T": 256, "B": 64, "synapses": int(len(c5["pre"])),
+        out["char_lm"] = {"custom_ms": ms_c5, "T": 256, "B": 64, "synapses": int(len(c5["pre"])),
                           "tokens_per_s": 64 * 256 / (ms_c5 / 1e3)}
+        if with_reference:
+            ms_r5 = _time_cuda(lm_reference, 1, 1)
+            rel5 = float((net.w_rec.grad - wr.grad).abs().max() / wr.grad.abs().max().clamp_min(1e-30))
+            out["char_lm"].update({"autograd_ms": ms_r5, "speedup": ms_r5 / ms_c5, "grad_rel_err": rel5})
     return out
 
 
@@ -553,6 +560,11 @@ def our_arm(args):
 
 def main():
     args = parse()
+    if args.leg:
+        legs = {"bptt": bptt_leg, "bptt-custom": lambda: bptt_leg(with_reference=False),
+                "configs": config_legs}
+        print(json.dumps({args.leg: legs[args.leg]()}), flush=True)
+        return 0
     if args.impl == "reference":
         return reference_arm(args)
     return our_arm(args)

@@ -28,8 +28,6 @@ import torch.nn.functional as F
 from . import _lib
 from ._lib import check, lib
 
-_FINALIZING = sys.is_finalizing  # kept: module globals are cleared at exit
-
 
 def _ptr(t):
     return C.c_void_p(t.data_ptr()) if t is not None else None
@@ -85,8 +83,9 @@ class SpikingCore:
             lib().snc_b200_bptt_release(self.h)
             self.h = None
 
-    def __del__(self):
-        if not _FINALIZING():  # the library may already be unloaded
+    def __del__(self, _finalizing=sys.is_finalizing):
+        # a default argument outlives the module globals cleared at exit
+        if not _finalizing():  # the library may already be unloaded
             self.release()
 
 

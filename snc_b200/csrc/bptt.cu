@@ -90,7 +90,7 @@ __device__ __forceinline__ void fwd_neuron(const BpArgs& a, int t, int j, float 
       my_d = a.in_d[eb + lane];
       my_w = a.w[a.in_eidx[eb + lane]];
     }
-    if (!SMOOTH) {
+    if constexpr (!SMOOTH) {
       // the spike words of kEdgeBatch edges are loaded together, then added
       // in edge order (the order of the sum is unchanged)
       for (int q0 = 0; q0 < n; q0 += kEdgeBatch<KB>) {
@@ -114,15 +114,13 @@ __device__ __forceinline__ void fwd_neuron(const BpArgs& a, int t, int j, float 
           for (int k = 0; k < KB; ++k)
             if ((wv[u][k] >> lane) & 1u) acc[k] = __fadd_rn(acc[k], wwv[u]);
       }
-      continue;
-    }
-    for (int q = 0; q < n; ++q) {
-      const int pre = __shfl_sync(0xffffffffu, my_pre, q);
-      const int d = __shfl_sync(0xffffffffu, my_d, q);
-      const float ww = __shfl_sync(0xffffffffu, my_w, q);
-      const int ts = t - d;
-      if (ts < 0) continue;
-      {
+    } else {
+      for (int q = 0; q < n; ++q) {
+        const int pre = __shfl_sync(0xffffffffu, my_pre, q);
+        const int d = __shfl_sync(0xffffffffu, my_d, q);
+        const float ww = __shfl_sync(0xffffffffu, my_w, q);
+        const int ts = t - d;
+        if (ts < 0) continue;
         const float* sp = a.spikes + ((size_t)ts * a.N + pre) * a.B;
 #pragma unroll
         for (int k = 0; k < KB; ++k) {

@@ -24,8 +24,6 @@ from ._lib import check, lib, ptr
 from .graph import INTERNAL, SNNGraph
 from .runtime import DeviceGraph, LIFParams, _events
 
-_FINALIZING = sys.is_finalizing  # kept: module globals are cleared at exit
-
 
 class EpropCfg(C.Structure):
     _fields_ = [("lr", C.c_float), ("w_max", C.c_float), ("surrogate_scale", C.c_float),
@@ -195,8 +193,9 @@ class CudaTrainSession:
             lib().snc_b200_eprop_release(self.h)
             self.h = None
 
-    def __del__(self):
-        if not _FINALIZING():  # the library may already be unloaded
+    def __del__(self, _finalizing=sys.is_finalizing):
+        # a default argument outlives the module globals cleared at exit
+        if not _finalizing():  # the library may already be unloaded
             self.release()
 
 

@@ -33,8 +33,6 @@ from ._lib import (MODE_ATOMIC, MODE_AUTO, MODE_BUCKET, MODE_SORT, PATH_AUTO, PA
                    ptr)
 from .graph import EVENT_DTYPE, SNNGraph
 
-_FINALIZING = sys.is_finalizing  # kept: module globals are cleared at exit
-
 BACKENDS = {
     "cuda-atomic": MODE_ATOMIC, "cuda-bucket": MODE_BUCKET, "cuda-sort": MODE_SORT,
     "b200-atomic": MODE_ATOMIC, "b200-bucket": MODE_BUCKET, "b200-sort": MODE_SORT,
@@ -126,8 +124,9 @@ class DeviceGraph:
             lib().snc_b200_graph_release(self.h)
             self.h = None
 
-    def __del__(self):
-        if not _FINALIZING():  # the library may already be unloaded
+    def __del__(self, _finalizing=sys.is_finalizing):
+        # a default argument outlives the module globals cleared at exit
+        if not _finalizing():  # the library may already be unloaded
             self.release()
 
 
@@ -192,8 +191,9 @@ class DeviceInputs:
             lib().snc_b200_inputs_release(self.h)
             self.h = None
 
-    def __del__(self):
-        if not _FINALIZING():  # the library may already be unloaded
+    def __del__(self, _finalizing=sys.is_finalizing):
+        # a default argument outlives the module globals cleared at exit
+        if not _finalizing():  # the library may already be unloaded
             self.release()
 
 
@@ -242,8 +242,9 @@ class Run:
             lib().snc_b200_run_release(self.h)
             self.h = None
 
-    def __del__(self):
-        if not _FINALIZING():  # the library may already be unloaded
+    def __del__(self, _finalizing=sys.is_finalizing):
+        # a default argument outlives the module globals cleared at exit
+        if not _finalizing():  # the library may already be unloaded
             self.release()
 
 

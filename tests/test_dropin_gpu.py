@@ -1,8 +1,10 @@
 """The reference's own CLIs with the B200 backend linked in place of its
 CUDA backends (snc_b200/adapter): snc_bench --compare-backends must report
 the cuda-* rows as served by the GPU (no "(fallback)") with the cpu
-backend's spike and event counts -- exactly for cuda-sort -- and snc_train
---device cuda must train on the GPU.  Skipped where the binaries were not
+backend's spike and event counts -- exactly for cuda-sort -- snc_train
+--device cuda must train on the GPU, and snc_cotrain --device cuda must run
+its e-prop rounds on the GPU and feed their activity statistics to the
+reference's structural update (Connectome::structural_update).  Skipped where the binaries were not
 built (they need the reference sources at build time)."""
 import os
 import re
@@ -15,6 +17,7 @@ BUILD = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
                      "adapter", "_build")
 BENCH = os.path.join(BUILD, "snc_bench")
 TRAIN = os.path.join(BUILD, "snc_train")
+COTRAIN = os.path.join(BUILD, "snc_cotrain")
 
 
 def compare(args):
@@ -64,3 +67,25 @@ def test_snc_train_device_cuda():
     assert last, out.stdout
     test_acc = float(last[0].split()[3])
     assert test_acc > 0.3, out.stdout  # chance is 0.1
+
+
+def test_snc_cotrain_device_cuda():
+    """cotrain_main.cpp:226-246: each round trains on the GPU session, carries
+    the weights back to the connectome and collects the per-synapse and
+    per-neuron activity the prune / regrow step consumes."""
+    if not os.path.exists(COTRAIN):
+        pytest.skip("reference CLIs not built")
+    out = subprocess.run([COTRAIN, "--device", "cuda", "--batch", "32", "--outer", "3", "--inner", "2",
+                          "--grow", "60", "--num-train", "512", "--num-test", "128", "--hidden", "128",
+                          "--structural-budget", "6000", "--lr", "1.0"],
+                         capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr
+    assert "device=cuda" in out.stdout and "fallback" not in out.stdout, out.stdout
+    rounds = [l.split() for l in out.stdout.splitlines() if re.match(r"^\s+\d+\s+\d+\s+\d+\s+\d+\s", l)]
+    assert len(rounds) == 3, out.stdout
+    synapses = {int(r[1]) for r in rounds}
+    assert len(synapses) == 1, out.stdout  # every pruned synapse regrown
+    for r in rounds[:2]:
+        assert int(r[2]) == 60 and int(r[3]) == 60, out.stdout
+    assert int(rounds[-1][6]) > 0, out.stdout  # the GPU forward spiked
+    assert float(rounds[-1][5]) > 0.2, out.stdout  # chance is 0.1

@@ -12,6 +12,7 @@ import pytest
 from oracle import oracle as O
 from snc_b200 import runtime as R
 from snc_b200 import workloads as W
+from snc_b200.graph import SNNGraph
 from tests.helpers import golden, spike_count_agreement, to_lif
 
 pytestmark = pytest.mark.gpu
@@ -175,5 +176,35 @@ def test_sort_bit_exact_at_the_largest_delay(pname, path, force):
     lif = R.LIFParams(threshold=1.0, decay=0.95, reset=0.0, refractory=1, reset_mode=1)
     ref = O.forward_batched(g, ev, steps, lif)
     assert int(ref["spikes"].sum()) > 0
+    out = run_gpu(g, ev, steps, lif, R.MODE_SORT, path, force_grid=force)
+    assert_exact(out, ref)
+
+
+@pytest.mark.parametrize("pname,path,force", PATHS)
+def test_sort_bit_exact_hub_columns(pname, path, force):
+    # 300 inputs onto 3 hidden neurons: hundreds of events reach one column in
+    # one step, so the ordered apply runs its long-list forms (chunks above
+    # the serial-link size, column lists longer than the register sort)
+    g = W.random_graph(23, n_in=300, n_hid=3, n_out=2, p=0.9, max_delay=3, recurrent=False)
+    ev, steps = W.random_events(24, g, 3, [40, 25, 33], rate=0.5)
+    lif = R.LIFParams(threshold=1.0, decay=0.9, reset=0.0, refractory=0, reset_mode=1)
+    ref = O.forward_batched(g, ev, steps, lif)
+    assert int(ref["events"].sum()) > 20000
+    out = run_gpu(g, ev, steps, lif, R.MODE_SORT, path, force_grid=force)
+    assert_exact(out, ref)
+
+
+@pytest.mark.parametrize("pname,path,force", PATHS)
+def test_graph_without_synapses(pname, path, force):
+    # inputs fire from their drive alone; nothing is delivered
+    N = 7
+    role = np.array([1, 1, 1, 1, 0, 2, 2], np.uint8)
+    channel = np.array([0, 1, 2, 2, -1, 0, 1], np.int32)
+    g = SNNGraph(N, np.zeros(N + 1, np.int32), np.zeros(0, np.int32), np.zeros(0, np.float32),
+                 np.zeros(0, np.int32), role, np.ones(N, np.int8), channel)
+    ev, steps = W.random_events(31, g, 2, [20, 9], rate=0.6)
+    lif = R.LIFParams(threshold=1.0, decay=0.9, refractory=1)
+    ref = O.forward_batched(g, ev, steps, lif)
+    assert int(ref["spikes"].sum()) > 0 and int(ref["events"].sum()) == 0
     out = run_gpu(g, ev, steps, lif, R.MODE_SORT, path, force_grid=force)
     assert_exact(out, ref)
