@@ -311,6 +311,13 @@ int snc_b200_bptt_backward(snc_b200_bptt* h, const float* w, const float* ext, i
                            int32_t smooth, const float* spikes, const uint32_t* spike_bits,
                            const float* v_saved, const float* grad_spikes, float* grad_w,
                            float* grad_ext, void* stream);
+/* Resident launches (default on): when one warp per neuron fits on the device
+ * and no neuron has more than 256 incoming or outgoing synapses, forward and
+ * backward stage every neuron's edges in shared memory for the whole launch
+ * and accumulate the weight gradients there; results are bit-identical to the
+ * global-memory form, which enable = 0 selects.  No reference counterpart
+ * (a tuning switch of this backend). */
+int snc_b200_bptt_set_resident(snc_b200_bptt* h, int32_t enable);
 /* Leaky integration along time (the leaky readouts of python/snc/shd_model.py:
  * 139-140 and python/snc/lm.py:90 as one kernel): x, y [T][n] fp32 device
  * tensors, y[t] = decay * y[t-1] + x[t] with y[-1] = 0, or with reverse != 0

@@ -85,6 +85,7 @@ SIGNATURES = {
     "snc_b200_eprop_collect_stats": (C.c_int, [P, P, P]),
     "snc_b200_bptt_create": (C.c_int, [I32, I32, P, P, P, P]),
     "snc_b200_bptt_release": (C.c_int, [P]),
+    "snc_b200_bptt_set_resident": (C.c_int, [P, I32]),
     "snc_b200_bptt_forward": (C.c_int, [P, P, P, I32, I32, C.c_float, C.c_float, C.c_float, I32,
                                         I32, P, P, P, P]),
     "snc_b200_bptt_backward": (C.c_int, [P, P, P, I32, I32, C.c_float, C.c_float, C.c_float, I32,

@@ -68,6 +68,11 @@ class SpikingCore:
         self.h = h
         self.perm_t = torch.as_tensor(self.perm, device=dev)
 
+    def set_resident(self, enable: bool) -> None:
+        """Allow (default) or forbid the resident launches that stage every
+        neuron's edges in shared memory; results are identical either way."""
+        check(lib().snc_b200_bptt_set_resident(self.h, int(bool(enable))), "bptt_set_resident")
+
     def to_csr(self, w):
         return w if self.identity else w[self.perm_t]
 

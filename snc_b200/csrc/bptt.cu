@@ -34,6 +34,8 @@
 
 struct snc_b200_bptt {
   int N = 0, S = 0, D = 1, R = 2, sm_count = 0;
+  int max_deg = 0;     // largest in- or out-degree
+  int resident = 1;    // allow resident launches
   int *row_ptr = nullptr, *out_post = nullptr, *out_d = nullptr;
   int *col_ptr = nullptr, *in_pre = nullptr, *in_d = nullptr, *in_eidx = nullptr;
   float *v = nullptr, *gv = nullptr, *gcur = nullptr, *seg = nullptr;
@@ -62,9 +64,64 @@ struct BpArgs {
   float* seg;          // [K][N][B]
   unsigned* ctl;
   int* err;
+  int res_cap;         // resident launches: edges per direction staged per warp
 };
 
 constexpr int kBpThreads = 256;
+constexpr int kResCapMax = 256;  // largest in / out degree a resident launch stages
+
+// A resident launch gives every warp one neuron for the whole launch and
+// stages that neuron's edges in shared memory once: incoming (pre, delay,
+// weight, CSR edge index, weight-gradient accumulator) in ascending CSR edge
+// order, outgoing (post, delay, weight) in CSR order.  The per-step edge
+// metadata loads and the global weight-gradient read-modify-writes leave the
+// time loop; the arithmetic and its order are those of the global-memory form.
+struct WarpEdges {
+  int *in_pre, *in_d, *in_eidx;
+  float *in_w, *in_acc;
+  int *out_post, *out_d;
+  float* out_w;
+  int nin, nout;
+};
+
+// Shared memory of a resident launch per warp: 8 arrays of res_cap entries.
+__device__ __forceinline__ WarpEdges warp_edges(float* base, int cap) {
+  const int wib = threadIdx.x >> 5;
+  int* p = reinterpret_cast<int*>(base) + (size_t)wib * 8 * cap;
+  WarpEdges we;
+  we.in_pre = p;
+  we.in_d = p + cap;
+  we.in_eidx = p + 2 * cap;
+  we.in_w = reinterpret_cast<float*>(p + 3 * cap);
+  we.in_acc = reinterpret_cast<float*>(p + 4 * cap);
+  we.out_post = p + 5 * cap;
+  we.out_d = p + 6 * cap;
+  we.out_w = reinterpret_cast<float*>(p + 7 * cap);
+  we.nin = we.nout = 0;
+  return we;
+}
+
+// Stage neuron i's edges (the whole warp; i < N).
+__device__ __forceinline__ void stage_edges(const BpArgs& a, int i, WarpEdges& we) {
+  const int lane = threadIdx.x & 31;
+  const int c0 = a.col_ptr[i], r0 = a.row_ptr[i];
+  we.nin = a.col_ptr[i + 1] - c0;
+  we.nout = a.row_ptr[i + 1] - r0;
+  for (int e = lane; e < we.nin; e += 32) {
+    we.in_pre[e] = a.in_pre[c0 + e];
+    we.in_d[e] = a.in_d[c0 + e];
+    const int ei = a.in_eidx[c0 + e];
+    we.in_eidx[e] = ei;
+    we.in_w[e] = a.w[ei];
+    we.in_acc[e] = 0.f;
+  }
+  for (int e = lane; e < we.nout; e += 32) {
+    we.out_post[e] = a.out_post[r0 + e];
+    we.out_d[e] = a.out_d[r0 + e];
+    we.out_w[e] = a.w[r0 + e];
+  }
+  __syncwarp();
+}
 
 // One step of the forward for neuron j.  v holds the neuron's state before
 // the step (per lane, batch elements lane + 32k) and is updated; vp receives
@@ -73,22 +130,22 @@ constexpr int kBpThreads = 256;
 template <int KB>
 constexpr int kEdgeBatch = KB >= 8 ? 4 : 8;
 
-template <int KB, bool SMOOTH>
+template <int KB, bool SMOOTH, bool RES>
 __device__ __forceinline__ void fwd_neuron(const BpArgs& a, int t, int j, float (&v)[KB],
-                                           float (&vp)[KB], float (&s)[KB]) {
+                                           float (&vp)[KB], float (&s)[KB], const WarpEdges& we) {
   const int lane = threadIdx.x & 31;
   float acc[KB];
 #pragma unroll
   for (int k = 0; k < KB; ++k) acc[k] = 0.f;
-  const int e0 = a.col_ptr[j], e1 = a.col_ptr[j + 1];
+  const int e0 = RES ? 0 : a.col_ptr[j], e1 = RES ? we.nin : a.col_ptr[j + 1];
   for (int eb = e0; eb < e1; eb += 32) {
     const int n = min(32, e1 - eb);
     int my_pre = 0, my_d = 1 << 30;
     float my_w = 0.f;
     if (lane < n) {
-      my_pre = a.in_pre[eb + lane];
-      my_d = a.in_d[eb + lane];
-      my_w = a.w[a.in_eidx[eb + lane]];
+      my_pre = RES ? we.in_pre[eb + lane] : a.in_pre[eb + lane];
+      my_d = RES ? we.in_d[eb + lane] : a.in_d[eb + lane];
+      my_w = RES ? we.in_w[eb + lane] : a.w[a.in_eidx[eb + lane]];
     }
     if constexpr (!SMOOTH) {
       // the spike words of kEdgeBatch edges are loaded together, then added
@@ -141,13 +198,19 @@ __device__ __forceinline__ void fwd_neuron(const BpArgs& a, int t, int j, float 
   }
 }
 
-template <int KB, bool SMOOTH>
+template <int KB, bool SMOOTH, bool RES>
 __global__ void __launch_bounds__(kBpThreads) k_bptt_forward(BpArgs a) {
+  extern __shared__ float sm_all[];
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int W = (gridDim.x * blockDim.x) >> 5;
   const unsigned nb = gridDim.x;
   unsigned target = 0;
+  WarpEdges we{};
+  if (RES) {
+    we = warp_edges(sm_all, a.res_cap);
+    if (gw < a.N) stage_edges(a, gw, we);
+  }
   for (int j = gw; j < a.N; j += W)
 #pragma unroll
     for (int k = 0; k < KB; ++k) {
@@ -162,7 +225,7 @@ __global__ void __launch_bounds__(kBpThreads) k_bptt_forward(BpArgs a) {
         const int b = 32 * k + lane;
         v[k] = b < a.B ? a.v[(size_t)j * a.B + b] : 0.f;
       }
-      fwd_neuron<KB, SMOOTH>(a, t, j, v, vp, s);
+      fwd_neuron<KB, SMOOTH, RES>(a, t, j, v, vp, s, we);
       const size_t plane = ((size_t)t * a.N + j) * a.B;
 #pragma unroll
       for (int k = 0; k < KB; ++k) {
@@ -185,9 +248,9 @@ __global__ void __launch_bounds__(kBpThreads) k_bptt_forward(BpArgs a) {
 
 // One backward step for neuron i; vp_plane points at the [N][B] plane of
 // pre-reset potentials of step t.  sm_g: this warp's [B] scratch.
-template <int KB, bool SMOOTH>
+template <int KB, bool SMOOTH, bool RES>
 __device__ __forceinline__ void bwd_neuron(const BpArgs& a, int t, int i, const float* vp_plane,
-                                           float* sm_g) {
+                                           float* sm_g, const WarpEdges& we) {
   const int lane = threadIdx.x & 31;
   const int N = a.N, B = a.B;
   float gs[KB];
@@ -198,15 +261,15 @@ __device__ __forceinline__ void bwd_neuron(const BpArgs& a, int t, int i, const 
     gs[k] = b < B ? a.gspk[plane + b] : 0.f;
   }
   // gradient reaching s_i(t) through every outgoing synapse (fires at t + d)
-  const int e0 = a.row_ptr[i], e1 = a.row_ptr[i + 1];
+  const int e0 = RES ? 0 : a.row_ptr[i], e1 = RES ? we.nout : a.row_ptr[i + 1];
   for (int eb = e0; eb < e1; eb += 32) {
     const int n = min(32, e1 - eb);
     int my_post = 0, my_d = 1 << 30;
     float my_w = 0.f;
     if (lane < n) {
-      my_post = a.out_post[eb + lane];
-      my_d = a.out_d[eb + lane];
-      my_w = a.w[eb + lane];
+      my_post = RES ? we.out_post[eb + lane] : a.out_post[eb + lane];
+      my_d = RES ? we.out_d[eb + lane] : a.out_d[eb + lane];
+      my_w = RES ? we.out_w[eb + lane] : a.w[eb + lane];
     }
     // the future gradients of kEdgeBatch edges are loaded together, then
     // accumulated in edge order
@@ -259,34 +322,63 @@ __device__ __forceinline__ void bwd_neuron(const BpArgs& a, int t, int i, const 
   }
   __syncwarp();
   // dL/dw for every incoming synapse: lane per synapse, sum of G over the
-  // samples whose pre neuron fired at t - d (only set bits are visited)
-  const int c0 = a.col_ptr[i], c1 = a.col_ptr[i + 1];
-  for (int e = c0 + lane; e < c1; e += 32) {
-    const int ts = t - a.in_d[e];
-    if (ts < 0) continue;
-    const int pre = a.in_pre[e];
-    float c = 0.f;
-    if (!SMOOTH) {
-      const uint32_t* wp = a.bits + ((size_t)ts * N + pre) * KB;
+  // samples whose pre neuron fired at t - d (only set bits are visited);
+  // the spike words of a lane's next two synapses are loaded together
+  const int c0 = RES ? 0 : a.col_ptr[i], c1 = RES ? we.nin : a.col_ptr[i + 1];
+  for (int e = c0 + lane; e < c1; e += 64) {
+    int ts[2], pre[2];
+    uint32_t wv[2][KB];
 #pragma unroll
-      for (int k = 0; k < KB; ++k) {
-        uint32_t word = wp[k];
-        while (word) {
-          const int bb = __ffs(word) - 1;
-          c = __fadd_rn(c, sm_g[32 * k + bb]);
-          word &= word - 1u;
-        }
+    for (int u = 0; u < 2; ++u) {
+      const int eu = e + 32 * u;
+      ts[u] = -1;
+      pre[u] = 0;
+      if (eu < c1) {
+        ts[u] = t - (RES ? we.in_d[eu] : a.in_d[eu]);
+        pre[u] = RES ? we.in_pre[eu] : a.in_pre[eu];
       }
-    } else {
-      const float* sp = a.spikes + ((size_t)ts * N + pre) * B;
-      for (int b = 0; b < B; ++b) c = __fadd_rn(c, __fmul_rn(sm_g[b], sp[b]));
+      if (!SMOOTH) {
+        const uint32_t* wp = a.bits + ((size_t)(ts[u] >= 0 ? ts[u] : 0) * N + pre[u]) * KB;
+#pragma unroll
+        for (int k = 0; k < KB; ++k) wv[u][k] = ts[u] >= 0 ? wp[k] : 0u;
+      }
     }
-    if (c != 0.f) a.gw[a.in_eidx[e]] = __fadd_rn(a.gw[a.in_eidx[e]], c);
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      if (ts[u] < 0) continue;
+      const int eu = e + 32 * u;
+      float c = 0.f;
+      if (!SMOOTH) {
+#pragma unroll
+        for (int k = 0; k < KB; ++k) {
+          uint32_t word = wv[u][k];
+          while (word) {
+            const int bb = __ffs(word) - 1;
+            c = __fadd_rn(c, sm_g[32 * k + bb]);
+            word &= word - 1u;
+          }
+        }
+      } else {
+        const float* sp = a.spikes + ((size_t)ts[u] * N + pre[u]) * B;
+        for (int b = 0; b < B; ++b) c = __fadd_rn(c, __fmul_rn(sm_g[b], sp[b]));
+      }
+      if (c != 0.f) {
+        if (RES) we.in_acc[eu] = __fadd_rn(we.in_acc[eu], c);
+        else a.gw[a.in_eidx[eu]] = __fadd_rn(a.gw[a.in_eidx[eu]], c);
+      }
+    }
   }
   __syncwarp();
 }
 
-template <int KB, bool SMOOTH>
+// Resident launches: the warp's weight gradients, accumulated in shared
+// memory in the order the global form adds them, go out once.
+__device__ __forceinline__ void flush_acc(const BpArgs& a, const WarpEdges& we) {
+  const int lane = threadIdx.x & 31;
+  for (int e = lane; e < we.nin; e += 32) a.gw[we.in_eidx[e]] = we.in_acc[e];
+}
+
+template <int KB, bool SMOOTH, bool RES>
 __global__ void __launch_bounds__(kBpThreads) k_bptt_backward(BpArgs a) {
   extern __shared__ float sm_all[];
   const int lane = threadIdx.x & 31;
@@ -297,6 +389,11 @@ __global__ void __launch_bounds__(kBpThreads) k_bptt_backward(BpArgs a) {
   const unsigned nb = gridDim.x;
   const size_t NB = (size_t)a.N * a.B;
   unsigned target = 0;
+  WarpEdges we{};
+  if (RES) {
+    we = warp_edges(sm_all + (size_t)(blockDim.x >> 5) * 32 * KB, a.res_cap);
+    if (gw < a.N) stage_edges(a, gw, we);
+  }
   for (int i = gw; i < a.N; i += W)
 #pragma unroll
     for (int k = 0; k < KB; ++k) {
@@ -305,10 +402,12 @@ __global__ void __launch_bounds__(kBpThreads) k_bptt_backward(BpArgs a) {
     }
   if (a.K == 0) {
     for (int t = a.T - 1; t >= 0; --t) {
-      for (int i = gw; i < a.N; i += W) bwd_neuron<KB, SMOOTH>(a, t, i, a.vsaved + (size_t)t * NB, sm_g);
+      for (int i = gw; i < a.N; i += W)
+        bwd_neuron<KB, SMOOTH, RES>(a, t, i, a.vsaved + (size_t)t * NB, sm_g, we);
       target += nb;
       if (!grid_sync(&a.ctl[0], target, a.err)) return;
     }
+    if (RES) flush_acc(a, we);
     return;
   }
   const int nseg = (a.T + a.K - 1) / a.K;
@@ -324,7 +423,7 @@ __global__ void __launch_bounds__(kBpThreads) k_bptt_backward(BpArgs a) {
         v[k] = (sg > 0 && b < a.B) ? a.vsaved[(size_t)(sg - 1) * NB + (size_t)i * a.B + b] : 0.f;
       }
       for (int t = t0; t < t1; ++t) {
-        fwd_neuron<KB, SMOOTH>(a, t, i, v, vp, s);
+        fwd_neuron<KB, SMOOTH, RES>(a, t, i, v, vp, s, we);
 #pragma unroll
         for (int k = 0; k < KB; ++k) {
           const int b = 32 * k + lane;
@@ -334,15 +433,31 @@ __global__ void __launch_bounds__(kBpThreads) k_bptt_backward(BpArgs a) {
     }
     for (int t = t1 - 1; t >= t0; --t) {
       for (int i = gw; i < a.N; i += W)
-        bwd_neuron<KB, SMOOTH>(a, t, i, a.seg + (size_t)(t - t0) * NB, sm_g);
+        bwd_neuron<KB, SMOOTH, RES>(a, t, i, a.seg + (size_t)(t - t0) * NB, sm_g, we);
       target += nb;
       if (!grid_sync(&a.ctl[0], target, a.err)) return;
     }
   }
+  if (RES) flush_acc(a, we);
 }
 
-template <typename F>
-static int coop_launch(F kern, const BpArgs& a, int sm_count, size_t smem, cudaStream_t st) {
+using BpKernel = void (*)(BpArgs);
+
+// Co-resident warps of a launch of kern with smem bytes per block.
+static int resident_warps(BpKernel kern, size_t smem, int sm_count) {
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBpThreads, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return per_sm * sm_count * (kBpThreads / 32);
+}
+
+static int coop_launch(BpKernel kern, const BpArgs& a, int sm_count, size_t smem, cudaStream_t st) {
   SNCB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   SNCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBpThreads, smem));
@@ -366,14 +481,24 @@ static int coop_launch(F kern, const BpArgs& a, int sm_count, size_t smem, cudaS
   return SNC_B200_OK;
 }
 
+template <int KB, bool RES>
+static BpKernel pick(bool forward, bool smooth) {
+  if (forward) return smooth ? k_bptt_forward<KB, true, RES> : k_bptt_forward<KB, false, RES>;
+  return smooth ? k_bptt_backward<KB, true, RES> : k_bptt_backward<KB, false, RES>;
+}
+
+// A resident launch (a.res_cap > 0) when one warp per neuron can be
+// co-resident with the staged edges, else the global-memory form.
 template <int KB>
-static int dispatch(bool forward, bool smooth, const BpArgs& a, int sm, cudaStream_t st) {
-  const size_t smem = (size_t)(kBpThreads / 32) * 32 * KB * sizeof(float);
-  if (forward)
-    return smooth ? coop_launch(k_bptt_forward<KB, true>, a, sm, 0, st)
-                  : coop_launch(k_bptt_forward<KB, false>, a, sm, 0, st);
-  return smooth ? coop_launch(k_bptt_backward<KB, true>, a, sm, smem, st)
-                : coop_launch(k_bptt_backward<KB, false>, a, sm, smem, st);
+static int dispatch(bool forward, bool smooth, BpArgs a, int sm, cudaStream_t st) {
+  const size_t smem = forward ? 0 : (size_t)(kBpThreads / 32) * 32 * KB * sizeof(float);
+  if (a.res_cap > 0) {
+    const size_t smem_r = smem + (size_t)(kBpThreads / 32) * 8 * a.res_cap * sizeof(int);
+    BpKernel kr = pick<KB, true>(forward, smooth);
+    if (resident_warps(kr, smem_r, sm) >= a.N) return coop_launch(kr, a, sm, smem_r, st);
+  }
+  a.res_cap = 0;
+  return coop_launch(pick<KB, false>(forward, smooth), a, sm, smem, st);
 }
 
 static int launch(bool forward, bool smooth, const BpArgs& a, int sm, cudaStream_t st) {
@@ -395,6 +520,12 @@ static int grow(T** p, size_t* cap, size_t n) {
   int rc = dev_alloc(p, n);
   if (!rc) *cap = n;
   return rc;
+}
+
+// Edges per direction a resident launch stages per warp (0: none).
+static int res_cap(const snc_b200_bptt* h) {
+  if (!h->resident || h->max_deg > kResCapMax) return 0;
+  return std::max(32, (h->max_deg + 31) / 32 * 32);
 }
 
 static int check_err(snc_b200_bptt* h, cudaStream_t st) {
@@ -458,6 +589,8 @@ int snc_b200_bptt_create(int32_t N, int32_t S, const int32_t* row_ptr, const int
   // incoming lists in ascending CSR edge order
   std::vector<int> col_ptr(N + 1, 0), in_pre(std::max(1, S)), in_d(std::max(1, S)), in_eidx(std::max(1, S));
   for (int e = 0; e < S; ++e) col_ptr[post[e] + 1]++;
+  for (int j = 0; j < N; ++j)
+    h->max_deg = std::max({h->max_deg, col_ptr[j + 1], row_ptr[j + 1] - row_ptr[j]});
   for (int j = 0; j < N; ++j) col_ptr[j + 1] += col_ptr[j];
   std::vector<int> fill(col_ptr.begin(), col_ptr.end() - 1);
   for (int i = 0; i < N; ++i)
@@ -482,6 +615,15 @@ int snc_b200_bptt_create(int32_t N, int32_t S, const int32_t* row_ptr, const int
     return rc;
   }
   *out = h;
+  return SNC_B200_OK;
+}
+
+int snc_b200_bptt_set_resident(snc_b200_bptt* h, int32_t enable) {
+  if (!h) {
+    set_error("bptt_set_resident: null handle");
+    return SNC_B200_EINVAL;
+  }
+  h->resident = enable != 0;
   return SNC_B200_OK;
 }
 
@@ -515,6 +657,7 @@ int snc_b200_bptt_forward(snc_b200_bptt* h, const float* w, const float* ext, in
   a.in_pre = h->in_pre; a.in_d = h->in_d; a.in_eidx = h->in_eidx;
   a.w = w; a.ext = ext; a.spikes = spikes; a.bits = spike_bits; a.vsaved = v_saved; a.v = h->v;
   a.ctl = h->ctl; a.err = h->err;
+  a.res_cap = res_cap(h);
   SNCB_CUDA(cudaMemsetAsync(h->ctl, 0, 16, st));
   SNCB_CUDA(cudaMemsetAsync(h->err, 0, 4, st));
   if ((rc = launch(true, smooth != 0, a, h->sm_count, st))) return rc;
@@ -547,6 +690,7 @@ int snc_b200_bptt_backward(snc_b200_bptt* h, const float* w, const float* ext, i
   a.bits = const_cast<uint32_t*>(spike_bits); a.vsaved = const_cast<float*>(v_saved); a.v = h->v;
   a.gspk = grad_spikes; a.gw = grad_w; a.gext = grad_ext; a.gv = h->gv; a.gcur = h->gcur; a.seg = h->seg;
   a.ctl = h->ctl; a.err = h->err;
+  a.res_cap = res_cap(h);
   SNCB_CUDA(cudaMemsetAsync(h->ctl, 0, 16, st));
   SNCB_CUDA(cudaMemsetAsync(h->err, 0, 4, st));
   SNCB_CUDA(cudaMemsetAsync(grad_w, 0, (size_t)std::max(1, h->S) * sizeof(float), st));

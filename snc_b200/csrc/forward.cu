@@ -155,19 +155,124 @@ __device__ __forceinline__ void apply_one(float* ring, int ring_stride, int col0
   }
 }
 
-// Tier S links chunks up to this many events in order with one warp; larger
-// chunks use unordered lists that every column sorts on its own.  Tier G
-// always links in order: its post blocks own hub columns whose per-step
-// event count can be large.
+// Chunks up to kCountMax events take the per-cell apply; above it tier S
+// links chunks up to kSerialLinkMax events in order with one warp and uses
+// unordered lists that every column sorts on its own beyond that, while tier
+// G always links in order (its post blocks own hub columns whose per-step
+// event count can be large).
+constexpr int kCountMax = 256;
 constexpr int kSerialLinkMax = 192;
 constexpr int kRegSort = 16;
 constexpr int kFirstFlag = 1 << 30;  // marks a group's first event of its column in st_col
+
+// Ordered apply of a small chunk (ce <= kCountMax <= blockDim.x, so thread q
+// owns staged event q) through its ring cells.  A hash table of kCellTable
+// keys (column, slot) -- zeroed by the caller before staging -- holds one
+// unordered list per cell (atomicExch heads, one link per event).  The first
+// arrival at a cell owns it: alone there, it applies its event; otherwise it
+// collects the cell's list (kCellSort entries in registers, sorted; longer
+// lists by repeated minimum selection) and applies it in order.  A step's
+// events spread over many more cells than columns -- a column's events carry
+// different delays -- so lists are short and no thread walks a hub column's
+// whole chain.
+constexpr int kCellTable = 2 * kCountMax;  // keys, then list heads (q + 1, 0 = empty)
+constexpr int kCellSort = 8;
+static_assert(2 * kCellTable <= kGChunk, "the table lives in st_next");
+static_assert(kCellTable + kCountMax <= kGChunk, "the links live in st_col beyond the chunk");
+
+// Enters staged event q of cell (c, sl) into the table; returns its entry.
+__device__ __forceinline__ unsigned cell_insert(int* tab, int* link, int q, int c, int sl, bool* first) {
+  unsigned* key = reinterpret_cast<unsigned*>(tab);
+  const unsigned k = (unsigned)c * 256u + (unsigned)sl + 1u;  // slot < 256, 0 = empty
+  unsigned h = (k * 2654435761u) >> 23;  // 9 bits: kCellTable = 512
+  // at most kCountMax = kCellTable / 2 keys: a free or equal entry is always found
+  for (int probe = 0; probe < kCellTable; ++probe) {
+    const unsigned old = atomicCAS(&key[h], 0u, k);
+    if (old == 0u || old == k) break;
+    h = (h + 1u) & (kCellTable - 1);
+  }
+  const int prev = atomicExch(&tab[kCellTable + h], q + 1);
+  link[q] = prev;
+  *first = prev == 0;
+  return h;
+}
+
+// The owner's part (after a barrier that follows every cell_insert): apply
+// the cell's events in increasing order -- their staging index, or with
+// KEYED their order key okey[x] (unique per event) -- then x.
+template <bool GLOBAL_RING, bool KEYED>
+__device__ __forceinline__ void cell_apply(const int* tab, const int* link, const int* okey,
+                                           const float* st_w, unsigned h, int q, int c, int sl,
+                                           float* ring, int ring_stride, int col0) {
+  const int top = tab[kCellTable + h];
+  if (top == q + 1) {
+    apply_one<GLOBAL_RING>(ring, ring_stride, col0, c, sl, st_w[q]);
+    return;
+  }
+  auto ord = [&](int x) -> long long {
+    return KEYED ? ((long long)okey[x] << 10) | x : (long long)x;  // x < kGChunk = 1024
+  };
+  long long r[kCellSort];
+#pragma unroll
+  for (int i = 0; i < kCellSort; ++i) r[i] = LLONG_MAX;
+  int p = top;
+#pragma unroll
+  for (int i = 0; i < kCellSort; ++i) {
+    if (p != 0) {
+      // insert into the sorted r (its largest entry is free)
+      r[kCellSort - 1] = ord(p - 1);
+#pragma unroll
+      for (int m = kCellSort - 1; m > 0; --m) {
+        const long long lo = min(r[m - 1], r[m]), hi = max(r[m - 1], r[m]);
+        r[m - 1] = lo;
+        r[m] = hi;
+      }
+      p = link[p - 1];
+    }
+  }
+  if (p == 0) {
+#pragma unroll
+    for (int i = 0; i < kCellSort; ++i)
+      if (r[i] != LLONG_MAX) apply_one<GLOBAL_RING>(ring, ring_stride, col0, c, sl, st_w[(int)(r[i] & 1023)]);
+    return;
+  }
+  long long last = -1;
+  for (;;) {
+    long long best = LLONG_MAX;
+    for (int x = top; x != 0; x = link[x - 1]) {
+      const long long o = ord(x - 1);
+      if (o > last && o < best) best = o;
+    }
+    if (best == LLONG_MAX) break;
+    apply_one<GLOBAL_RING>(ring, ring_stride, col0, c, sl, st_w[(int)(best & 1023)]);
+    last = best;
+  }
+}
+
+template <bool GLOBAL_RING>
+__device__ void apply_cells(int ce, int* tab, int* st_col, const int* st_slot, const float* st_w,
+                            float* ring, int ring_stride, int col0) {
+  int* link = st_col + kCellTable;
+  const int q = threadIdx.x;
+  int c = 0, sl = 0;
+  unsigned h = 0;
+  bool first = false;
+  if (q < ce) {
+    c = st_col[q];
+    sl = st_slot[q];
+    h = cell_insert(tab, link, q, c, sl, &first);
+  }
+  __syncthreads();
+  if (first) cell_apply<GLOBAL_RING, false>(tab, link, nullptr, st_w, h, q, c, sl, ring, ring_stride, col0);
+  __syncthreads();
+}
 
 // Ordered apply of one chunk of staged events.  Staging index q is the
 // (pre, edge) order of the CPU backend.  The events were staged with their
 // block-local column st_col[q] (head / tail of every local column = -1).
 // Every ring cell must receive its contributions in increasing q.
-//  - small chunks: every warp links the events of its 32-event groups
+//  - chunks up to kCountMax events: apply_cells (above);
+//  - chunks up to serial_max: every warp links the events of its 32-event groups
 //    (match.any: successor within the group, first event of each column
 //    flagged), then one warp joins the groups in staging order through the
 //    column tails -- one shared-memory round trip per group; one thread per
@@ -182,6 +287,10 @@ __device__ void apply_ordered(int ce, int* head, int* tail, int ncols_local, int
                               const int* st_slot, const float* st_w, int* st_next, float* ring,
                               int ring_stride, int col0, int serial_max) {
   __syncthreads();
+  if (ce <= kCountMax && ce <= (int)blockDim.x) {
+    apply_cells<GLOBAL_RING>(ce, st_next, st_col, st_slot, st_w, ring, ring_stride, col0);
+    return;
+  }
   if (ce > serial_max) {
     for (int q = threadIdx.x; q < ce; q += blockDim.x) st_next[q] = atomicExch(&head[st_col[q]], q);
     __syncthreads();
@@ -444,8 +553,9 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
             st_slot[qq] = ring_slot(s0, edge_delay(ed), R);
             st_w[qq] = edge_w(ed);
             st_col[qq] = edge_col(ed);
-            st_next[qq] = -1;
           }
+          if (ce <= kCountMax)  // apply_cells' table (st_next has CH = 1024 entries)
+            for (int i = tid; i < 2 * kCellTable; i += nthr) st_next[i] = 0;
           __syncthreads();
           apply_ordered<false>(ce, head, tail, nc, st_col, st_slot, st_w, st_next, ring, nc, 0,
                                kSerialLinkMax);
@@ -765,12 +875,81 @@ __device__ void phase_b_scan(const FwdArgs& a, const GSmem& sm, int* scratch, in
         sm.st_slot[qq] = ring_slot(s0, edge_delay(ed), R);
         sm.st_w[qq] = edge_w(ed);
         sm.st_col[qq] = edge_col(ed) - cb0;
-        sm.st_next[qq] = -1;
       }
+      if (ce <= kCountMax)  // apply_cells' table
+        for (int i = tid; i < 2 * kCellTable; i += nthr) sm.st_next[i] = 0;
       apply_ordered<!RSM>(ce, sm.head, sm.tail, cb1 - cb0, sm.st_col, sm.st_slot, sm.st_w,
                           sm.st_next, rb, stride, col0, kGChunk);
     }
   }
+}
+
+// Phase B for at most 32 inbox descriptors (the common step): warp 0 holds
+// them from the speculative read and scans their lengths with shuffles (no
+// rank pass).  BUCKET accumulates straight away; SORT stages each event with
+// its gedges index as order key -- within one destination block the gedges
+// order is the (pre, edge) order of the CPU backend, since gedges keeps the
+// CSR row order and regroups each row stably by destination block -- and
+// applies it per ring cell (cell_insert / cell_apply) with no descriptor sort.
+// Returns false, with nothing applied, for a SORT step of more than
+// kCountMax events: the general path takes it.
+template <int MODE, bool RSM>
+__device__ bool phase_b_fast(const FwdArgs& a, const GSmem& sm, int k, int t, int cb0, int cnt,
+                             unsigned long long spec) {
+  __shared__ int s_E;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  if (tid < 32) {
+    const unsigned long long dsc = tid < cnt ? spec : 0ull;
+    const int len = (int)(dsc & 0xffffffffu);
+    int incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (tid >= o) incl += y;
+    }
+    if (tid < cnt) {
+      sm.desc[tid] = dsc;
+      sm.seg_p[tid] = incl - len;
+    }
+    if (tid == 31) s_E = incl;
+  }
+  if (MODE == MODE_SORT)
+    for (int i = tid; i < 2 * kCellTable; i += nthr) sm.st_next[i] = 0;
+  __syncthreads();
+  const int E = s_E;
+  if (MODE == MODE_SORT && E > kCountMax) return false;
+  const int R = a.R, s0 = t % R;
+  float* rb = ring_base<RSM>(a, sm, k);
+  const int stride = RSM ? a.BS : a.ncols;
+  const int col0 = RSM ? 0 : cb0;
+  if (MODE == MODE_BUCKET) {
+    for (int qq = tid; qq < E; qq += nthr) {
+      const int d = upper_index(sm.seg_p, cnt, qq);
+      const uint2 ed = a.gedges[(int)(sm.desc[d] >> 32) + (qq - sm.seg_p[d])];
+      const int cidx = RSM ? edge_col(ed) - cb0 : edge_col(ed);
+      atomicAdd(&rb[(size_t)ring_slot(s0, edge_delay(ed), R) * stride + cidx], edge_w(ed));
+    }
+    __syncthreads();
+    return true;
+  }
+  const int q = tid;  // E <= kCountMax <= blockDim.x
+  int c = 0, sl = 0;
+  unsigned h = 0;
+  bool first = false;
+  if (q < E) {
+    const int d = upper_index(sm.seg_p, cnt, q);
+    const int edge = (int)(sm.desc[d] >> 32) + (q - sm.seg_p[d]);
+    const uint2 ed = a.gedges[edge];
+    sl = ring_slot(s0, edge_delay(ed), R);
+    c = edge_col(ed) - cb0;
+    sm.st_w[q] = edge_w(ed);
+    sm.st_slot[q] = edge;  // order key
+    h = cell_insert(sm.st_next, sm.st_col, q, c, sl, &first);
+  }
+  __syncthreads();
+  if (first) cell_apply<!RSM, true>(sm.st_next, sm.st_col, sm.st_slot, sm.st_w, h, q, c, sl, rb, stride, col0);
+  __syncthreads();
+  return true;
 }
 
 // Phase B (BUCKET / SORT): as owner of the ring columns of block b, expand
@@ -799,6 +978,7 @@ __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, 
   __syncthreads();
   const int cnt = s_cnt;
   if (cnt == 0) return;
+  if (cnt <= 32 && phase_b_fast<MODE, RSM>(a, sm, k, t, cb0, cnt, spec)) return;
   if (MODE == MODE_SORT && cnt > kGDesc) {
     phase_b_scan<RSM>(a, sm, scratch, k, t, b, cb0, cb1);
     return;
@@ -870,10 +1050,11 @@ __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, 
           sm.st_slot[qq] = slot;
           sm.st_w[qq] = edge_w(ed);
           sm.st_col[qq] = edge_col(ed) - cb0;
-          sm.st_next[qq] = -1;
         }
       }
       if (MODE == MODE_SORT) {
+        if (ce <= kCountMax)  // apply_cells' table
+          for (int i = tid; i < 2 * kCellTable; i += nthr) sm.st_next[i] = 0;
         apply_ordered<!RSM>(ce, sm.head, sm.tail, cb1 - cb0, sm.st_col, sm.st_slot, sm.st_w,
                             sm.st_next, rb, stride, col0, kGChunk);
       } else {

@@ -212,3 +212,51 @@ def test_delayed_snn_readout_and_gradients():
     rel_close(net.w.grad.cpu(), wt.grad, 1e-4)
     rel_close(net.readout.weight.grad.cpu(), wro.grad, 1e-4)
     rel_close(net.readout.bias.grad.cpu(), bro.grad, 1e-4)
+
+
+def _run_core(g, w, ext, proj, ckpt, smooth, resident):
+    core = BP.SpikingCore(g.num_neurons, g.pre_ids(), g.post_ids, g.delays, device=DEV)
+    core.set_resident(resident)
+    wt = torch.as_tensor(w, device=DEV).clone().requires_grad_(True)
+    et = ext.to(DEV).clone().requires_grad_(True)
+    s = BP.spiking_core(wt, et, core, 1.0, 0.9, 8.0, ckpt, smooth)
+    (s * proj.to(DEV)).sum().backward()
+    return s.detach().cpu(), wt.grad.cpu(), et.grad.cpu()
+
+
+@pytest.mark.parametrize("smooth", [False, True])
+@pytest.mark.parametrize("ckpt", [0, 4])
+def test_resident_launch_is_bit_identical(smooth, ckpt):
+    # edges staged in shared memory per warp against the global-memory form
+    g, w = graph(7, n_hid=90)
+    T, B = 19, 40
+    gen = torch.Generator().manual_seed(3)
+    ext = (torch.rand(T, B, g.num_neurons, generator=gen) < 0.3).float() * 1.2
+    proj = torch.randn(T, B, g.num_neurons, generator=gen)
+    a = _run_core(g, w, ext, proj, ckpt, smooth, True)
+    b = _run_core(g, w, ext, proj, ckpt, smooth, False)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x.numpy().view(np.uint32), y.numpy().view(np.uint32))
+
+
+def test_hub_neuron_beyond_the_resident_limit():
+    # one neuron with 300 outgoing and one with 300 incoming synapses: the
+    # launch falls back to the global-memory form; still exact / within 1e-4
+    rng = np.random.default_rng(5)
+    N = 340
+    pre = np.concatenate([np.zeros(300, np.int64), rng.integers(1, N, 300), rng.integers(0, N, 600)])
+    post = np.concatenate([rng.integers(1, N, 300), np.full(300, 5), rng.integers(0, N, 600)])
+    d = rng.integers(1, 4, pre.shape[0])
+    from snc_b200.graph import from_edges
+    role = np.zeros(N, np.uint8)
+    g = from_edges(N, pre, post, np.ones(pre.shape[0], np.float32), d, role)
+    w = (rng.normal(0, 0.3, g.num_synapses)).astype(np.float32)
+    T, B = 12, 33
+    gen = torch.Generator().manual_seed(9)
+    ext = (torch.rand(T, B, N, generator=gen) < 0.3).float() * 1.1
+    proj = torch.randn(T, B, N, generator=gen)
+    s, gw, ge = gpu_run(g, w, ext, 1.0, 0.9, 8.0, proj, 4)
+    rs, rgw, rge = ref_run(g, w, ext, 1.0, 0.9, 8.0, proj)
+    np.testing.assert_array_equal(s.numpy(), rs.numpy())
+    rel_close(gw, rgw)
+    rel_close(ge, rge)
