@@ -156,12 +156,10 @@ __device__ __forceinline__ void apply_one(float* ring, int ring_stride, int col0
 }
 
 // Chunks up to kCountMax events take the per-cell apply; above it tier S
-// links chunks up to kSerialLinkMax events in order with one warp and uses
-// unordered lists that every column sorts on its own beyond that, while tier
-// G always links in order (its post blocks own hub columns whose per-step
-// event count can be large).
+// uses unordered lists that every column sorts on its own, while tier G links
+// in order (its post blocks own hub columns whose per-step event count can be
+// large).
 constexpr int kCountMax = 256;
-constexpr int kSerialLinkMax = 192;
 constexpr int kRegSort = 16;
 constexpr int kFirstFlag = 1 << 30;  // marks a group's first event of its column in st_col
 
@@ -558,7 +556,7 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
             for (int i = tid; i < 2 * kCellTable; i += nthr) st_next[i] = 0;
           __syncthreads();
           apply_ordered<false>(ce, head, tail, nc, st_col, st_slot, st_w, st_next, ring, nc, 0,
-                               kSerialLinkMax);
+                               kCountMax);
           __syncthreads();
         }
       }
