@@ -68,6 +68,11 @@ struct BpArgs {
 };
 
 constexpr int kBpThreads = 256;
+// Blocks per SM the kernels are compiled for: one warp per neuron has to stay
+// co-resident (4096 neurons need 4 blocks of 8 warps on each of 148 SMs), so
+// narrow batches keep to 64 registers.
+template <int KB>
+constexpr int kBpMinBlocks = KB <= 2 ? 4 : (KB <= 4 ? 2 : 1);
 constexpr int kResCapMax = 256;  // largest in / out degree a resident launch stages
 
 // A resident launch gives every warp one neuron for the whole launch and
@@ -199,7 +204,7 @@ __device__ __forceinline__ void fwd_neuron(const BpArgs& a, int t, int j, float 
 }
 
 template <int KB, bool SMOOTH, bool RES>
-__global__ void __launch_bounds__(kBpThreads) k_bptt_forward(BpArgs a) {
+__global__ void __launch_bounds__(kBpThreads, kBpMinBlocks<KB>) k_bptt_forward(BpArgs a) {
   extern __shared__ float sm_all[];
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -261,6 +266,7 @@ __device__ __forceinline__ void bwd_neuron(const BpArgs& a, int t, int i, const 
     gs[k] = b < B ? a.gspk[plane + b] : 0.f;
   }
   // gradient reaching s_i(t) through every outgoing synapse (fires at t + d)
+  const int tr = t % a.R;
   const int e0 = RES ? 0 : a.row_ptr[i], e1 = RES ? we.nout : a.row_ptr[i + 1];
   for (int eb = e0; eb < e1; eb += 32) {
     const int n = min(32, e1 - eb);
@@ -271,6 +277,15 @@ __device__ __forceinline__ void bwd_neuron(const BpArgs& a, int t, int i, const 
       my_d = RES ? we.out_d[eb + lane] : a.out_d[eb + lane];
       my_w = RES ? we.out_w[eb + lane] : a.w[eb + lane];
     }
+    // each lane turns its own edge into an offset into the ring of future
+    // gradients (slot of t + d: one conditional subtraction, d < R) and a
+    // validity bit; the batches below only broadcast them
+    const unsigned okm = __ballot_sync(0xffffffffu, lane < n && t + my_d < a.T);
+    size_t my_off = 0;
+    if ((okm >> lane) & 1u) {
+      const int slot = tr + my_d >= a.R ? tr + my_d - a.R : tr + my_d;
+      my_off = ((size_t)slot * N + my_post) * B;
+    }
     // the future gradients of kEdgeBatch edges are loaded together, then
     // accumulated in edge order
     for (int q0 = 0; q0 < n; q0 += kEdgeBatch<KB>) {
@@ -279,13 +294,12 @@ __device__ __forceinline__ void bwd_neuron(const BpArgs& a, int t, int i, const 
       bool okv[kEdgeBatch<KB>];
 #pragma unroll
       for (int u = 0; u < kEdgeBatch<KB>; ++u) {
-        const int q = q0 + u;
-        const int post = __shfl_sync(0xffffffffu, my_post, q & 31);
-        const int d = __shfl_sync(0xffffffffu, my_d, q & 31);
-        wwv[u] = __shfl_sync(0xffffffffu, my_w, q & 31);
-        const int tt = t + d;
-        okv[u] = q < n && tt < a.T;
-        const float* gp = a.gcur + ((size_t)(okv[u] ? tt % a.R : 0) * N + post) * B;
+        const int src = (q0 + u) & 31;  // q0 + u < 32: kEdgeBatch divides 32
+        const unsigned olo = __shfl_sync(0xffffffffu, (unsigned)my_off, src);
+        const unsigned ohi = __shfl_sync(0xffffffffu, (unsigned)(my_off >> 32), src);
+        wwv[u] = __shfl_sync(0xffffffffu, my_w, src);
+        okv[u] = (okm >> src) & 1u;
+        const float* gp = a.gcur + (((size_t)ohi << 32) | olo);
 #pragma unroll
         for (int k = 0; k < KB; ++k) {
           const int b = 32 * k + lane;
@@ -302,7 +316,7 @@ __device__ __forceinline__ void bwd_neuron(const BpArgs& a, int t, int i, const 
           }
     }
   }
-  float* gc = a.gcur + ((size_t)(t % a.R) * N + i) * B;
+  float* gc = a.gcur + ((size_t)tr * N + i) * B;
 #pragma unroll
   for (int k = 0; k < KB; ++k) {
     const int b = 32 * k + lane;
@@ -379,7 +393,7 @@ __device__ __forceinline__ void flush_acc(const BpArgs& a, const WarpEdges& we) 
 }
 
 template <int KB, bool SMOOTH, bool RES>
-__global__ void __launch_bounds__(kBpThreads) k_bptt_backward(BpArgs a) {
+__global__ void __launch_bounds__(kBpThreads, kBpMinBlocks<KB>) k_bptt_backward(BpArgs a) {
   extern __shared__ float sm_all[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
