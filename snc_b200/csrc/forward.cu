@@ -178,18 +178,25 @@ constexpr int kCellSort = 8;
 static_assert(2 * kCellTable <= kGChunk, "the table lives in st_next");
 static_assert(kCellTable + kCountMax <= kGChunk, "the links live in st_col beyond the chunk");
 
-// Enters staged event q of cell (c, sl) into the table; returns its entry.
+// Table sizes (keys; as many list heads follow) and their hash bits.
+template <int TS>
+constexpr int kTabBits = TS == 1024 ? 10 : 9;
+
+// Enters staged event q of cell (c, sl) into a table of TS keys (at most TS / 2
+// distinct cells); returns its entry.
+template <int TS>
 __device__ __forceinline__ unsigned cell_insert(int* tab, int* link, int q, int c, int sl, bool* first) {
+  static_assert(TS == 512 || TS == 1024, "table size");
   unsigned* key = reinterpret_cast<unsigned*>(tab);
   const unsigned k = (unsigned)c * 256u + (unsigned)sl + 1u;  // slot < 256, 0 = empty
-  unsigned h = (k * 2654435761u) >> 23;  // 9 bits: kCellTable = 512
-  // at most kCountMax = kCellTable / 2 keys: a free or equal entry is always found
-  for (int probe = 0; probe < kCellTable; ++probe) {
+  unsigned h = (k * 2654435761u) >> (32 - kTabBits<TS>);
+  // at most TS / 2 keys: a free or equal entry is always found
+  for (int probe = 0; probe < TS; ++probe) {
     const unsigned old = atomicCAS(&key[h], 0u, k);
     if (old == 0u || old == k) break;
-    h = (h + 1u) & (kCellTable - 1);
+    h = (h + 1u) & (TS - 1);
   }
-  const int prev = atomicExch(&tab[kCellTable + h], q + 1);
+  const int prev = atomicExch(&tab[TS + h], q + 1);
   link[q] = prev;
   *first = prev == 0;
   return h;
@@ -198,11 +205,11 @@ __device__ __forceinline__ unsigned cell_insert(int* tab, int* link, int q, int 
 // The owner's part (after a barrier that follows every cell_insert): apply
 // the cell's events in increasing order -- their staging index, or with
 // KEYED their order key okey[x] (unique per event) -- then x.
-template <bool GLOBAL_RING, bool KEYED>
+template <bool GLOBAL_RING, bool KEYED, int TS>
 __device__ __forceinline__ void cell_apply(const int* tab, const int* link, const int* okey,
                                            const float* st_w, unsigned h, int q, int c, int sl,
                                            float* ring, int ring_stride, int col0) {
-  const int top = tab[kCellTable + h];
+  const int top = tab[TS + h];
   if (top == q + 1) {
     apply_one<GLOBAL_RING>(ring, ring_stride, col0, c, sl, st_w[q]);
     return;
@@ -258,10 +265,12 @@ __device__ void apply_cells(int ce, int* tab, int* st_col, const int* st_slot, c
   if (q < ce) {
     c = st_col[q];
     sl = st_slot[q];
-    h = cell_insert(tab, link, q, c, sl, &first);
+    h = cell_insert<kCellTable>(tab, link, q, c, sl, &first);
   }
   __syncthreads();
-  if (first) cell_apply<GLOBAL_RING, false>(tab, link, nullptr, st_w, h, q, c, sl, ring, ring_stride, col0);
+  if (first)
+    cell_apply<GLOBAL_RING, false, kCellTable>(tab, link, nullptr, st_w, h, q, c, sl, ring, ring_stride,
+                                               col0);
   __syncthreads();
 }
 
@@ -797,7 +806,8 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, unsigne
       }
     }
   }
-  __syncthreads();
+  // no closing barrier: every caller's next step starts with one (the next
+  // slot's phase A, grid_arrive, or the end of the launch)
 }
 
 // Ring view of one wave slot for the post-owner phase: shared-memory slice
@@ -882,40 +892,57 @@ __device__ void phase_b_scan(const FwdArgs& a, const GSmem& sm, int* scratch, in
   }
 }
 
-// Phase B for at most 32 inbox descriptors (the common step): warp 0 holds
-// them from the speculative read and scans their lengths with shuffles (no
-// rank pass).  BUCKET accumulates straight away; SORT stages each event with
-// its gedges index as order key -- within one destination block the gedges
-// order is the (pre, edge) order of the CPU backend, since gedges keeps the
-// CSR row order and regroups each row stably by destination block -- and
-// applies it per ring cell (cell_insert / cell_apply) with no descriptor sort.
-// Returns false, with nothing applied, for a SORT step of more than
-// kCountMax events: the general path takes it.
+// Phase B for at most 64 inbox descriptors (SORT; 32 for BUCKET) -- the
+// common step: warp 0 holds them from the speculative read (lane l:
+// descriptors l and l + 32) and scans
+// their lengths with shuffles (no rank pass).  BUCKET accumulates straight
+// away; SORT stages each event with its gedges index as order key -- within
+// one destination block the gedges order is the (pre, edge) order of the CPU
+// backend, since gedges keeps the CSR row order and regroups each row stably
+// by destination block -- and applies it per ring cell (cell_insert /
+// cell_apply with a 1024-key table in the descriptor buffer) with no
+// descriptor sort.  Returns false, with nothing applied, for a SORT step of
+// more than kFastMax events: the general path takes it.
+constexpr int kFastDesc = 64;
+constexpr int kFastMax = 512;
+static_assert(2 * 2 * kFastMax * sizeof(int) <= kGDesc * sizeof(unsigned long long),
+              "the fast path's table lives in the descriptor buffer");
+
 template <int MODE, bool RSM>
 __device__ bool phase_b_fast(const FwdArgs& a, const GSmem& sm, int k, int t, int cb0, int cnt,
-                             unsigned long long spec) {
+                             unsigned long long spec, unsigned long long spec2, bool tail_sync) {
   __shared__ int s_E;
   const int tid = threadIdx.x, nthr = blockDim.x;
+  int* tab = reinterpret_cast<int*>(sm.desc);
   if (tid < 32) {
-    const unsigned long long dsc = tid < cnt ? spec : 0ull;
-    const int len = (int)(dsc & 0xffffffffu);
-    int incl = len;
+    const unsigned long long d0 = tid < cnt ? spec : 0ull;
+    const unsigned long long d1 = MODE == MODE_SORT && tid + 32 < cnt ? spec2 : 0ull;
+    const int l0 = (int)(d0 & 0xffffffffu), l1 = (int)(d1 & 0xffffffffu);
+    int i0 = l0, i1 = l1;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, incl, o);
-      if (tid >= o) incl += y;
+      const int y0 = __shfl_up_sync(0xffffffffu, i0, o), y1 = __shfl_up_sync(0xffffffffu, i1, o);
+      if (tid >= o) {
+        i0 += y0;
+        i1 += y1;
+      }
     }
+    const int t0 = __shfl_sync(0xffffffffu, i0, 31);
     if (tid < cnt) {
-      sm.desc[tid] = dsc;
-      sm.seg_p[tid] = incl - len;
+      sm.dsort[tid] = d0;
+      sm.seg_p[tid] = i0 - l0;
     }
-    if (tid == 31) s_E = incl;
+    if (tid + 32 < cnt) {
+      sm.dsort[tid + 32] = d1;
+      sm.seg_p[tid + 32] = t0 + i1 - l1;
+    }
+    if (tid == 31) s_E = t0 + i1;
   }
   if (MODE == MODE_SORT)
-    for (int i = tid; i < 2 * kCellTable; i += nthr) sm.st_next[i] = 0;
+    for (int i = tid; i < 2 * 2 * kFastMax; i += nthr) tab[i] = 0;
   __syncthreads();
   const int E = s_E;
-  if (MODE == MODE_SORT && E > kCountMax) return false;
+  if (MODE == MODE_SORT && (E > kFastMax || E > nthr)) return false;
   const int R = a.R, s0 = t % R;
   float* rb = ring_base<RSM>(a, sm, k);
   const int stride = RSM ? a.BS : a.ncols;
@@ -923,39 +950,44 @@ __device__ bool phase_b_fast(const FwdArgs& a, const GSmem& sm, int k, int t, in
   if (MODE == MODE_BUCKET) {
     for (int qq = tid; qq < E; qq += nthr) {
       const int d = upper_index(sm.seg_p, cnt, qq);
-      const uint2 ed = a.gedges[(int)(sm.desc[d] >> 32) + (qq - sm.seg_p[d])];
+      const uint2 ed = a.gedges[(int)(sm.dsort[d] >> 32) + (qq - sm.seg_p[d])];
       const int cidx = RSM ? edge_col(ed) - cb0 : edge_col(ed);
       atomicAdd(&rb[(size_t)ring_slot(s0, edge_delay(ed), R) * stride + cidx], edge_w(ed));
     }
-    __syncthreads();
+    if (tail_sync) __syncthreads();
     return true;
   }
-  const int q = tid;  // E <= kCountMax <= blockDim.x
+  const int q = tid;  // E <= blockDim.x
   int c = 0, sl = 0;
   unsigned h = 0;
   bool first = false;
   if (q < E) {
     const int d = upper_index(sm.seg_p, cnt, q);
-    const int edge = (int)(sm.desc[d] >> 32) + (q - sm.seg_p[d]);
+    const int edge = (int)(sm.dsort[d] >> 32) + (q - sm.seg_p[d]);
     const uint2 ed = a.gedges[edge];
     sl = ring_slot(s0, edge_delay(ed), R);
     c = edge_col(ed) - cb0;
     sm.st_w[q] = edge_w(ed);
     sm.st_slot[q] = edge;  // order key
-    h = cell_insert(sm.st_next, sm.st_col, q, c, sl, &first);
+    h = cell_insert<2 * kFastMax>(tab, sm.st_col, q, c, sl, &first);
   }
   __syncthreads();
-  if (first) cell_apply<!RSM, true>(sm.st_next, sm.st_col, sm.st_slot, sm.st_w, h, q, c, sl, rb, stride, col0);
-  __syncthreads();
+  if (first)
+    cell_apply<!RSM, true, 2 * kFastMax>(tab, sm.st_col, sm.st_slot, sm.st_w, h, q, c, sl, rb, stride,
+                                         col0);
+  if (tail_sync) __syncthreads();
   return true;
 }
 
 // Phase B (BUCKET / SORT): as owner of the ring columns of block b, expand
 // this step's inbox descriptors and accumulate them into the block's ring
 // slice -- unordered (BUCKET) or per ring cell in (pre, edge) order (SORT).
+// tail_sync: close with a barrier (another phase B of this step follows;
+// otherwise the caller's next step -- phase A, the end of the wave or of the
+// launch -- starts with one).
 template <int MODE, bool RSM>
 __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, int t, int b,
-                        int cb0, int cb1) {
+                        int cb0, int cb1, bool tail_sync) {
   __shared__ int s_cnt;
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int R = a.R;
@@ -966,8 +998,9 @@ __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, 
   // read the first descriptor slots in the same round trip as the count
   // (slots beyond the count hold stale descriptors and are ignored)
   const int cap = sm.ib[b + 1] - sm.ib[b];
-  unsigned long long spec = 0;
+  unsigned long long spec = 0, spec2 = 0;
   if (tid < kGDesc && tid < cap) spec = __ldcg(&box[tid]);
+  if (MODE == MODE_SORT && tid < 32 && tid + 32 < cap) spec2 = __ldcg(&box[tid + 32]);
   if (tid == 0) {
     s_cnt = __ldcg(cntp);
     // reset for step t + 2 (written again only after the next grid barrier)
@@ -976,7 +1009,9 @@ __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, 
   __syncthreads();
   const int cnt = s_cnt;
   if (cnt == 0) return;
-  if (cnt <= 32 && phase_b_fast<MODE, RSM>(a, sm, k, t, cb0, cnt, spec)) return;
+  if (cnt <= (MODE == MODE_SORT ? kFastDesc : 32) &&
+      phase_b_fast<MODE, RSM>(a, sm, k, t, cb0, cnt, spec, spec2, tail_sync))
+    return;
   if (MODE == MODE_SORT && cnt > kGDesc) {
     phase_b_scan<RSM>(a, sm, scratch, k, t, b, cb0, cb1);
     return;
@@ -1134,7 +1169,11 @@ __global__ void __launch_bounds__(kGThreadsMax, 1) k_tier_g(FwdArgs a) {
       if (!grid_wait(&a.ctl[0], target, a.err)) return;
       if (MODE != MODE_ATOMIC)
         for (int k = 0; k < nk; ++k)
-          if (t < s_T[k]) phase_b<MODE, RSM>(a, sm, scratch, k, t, b, cb0, cb1);
+          if (t < s_T[k]) {
+            bool more = false;
+            for (int k2 = k + 1; k2 < nk; ++k2) more |= t < s_T[k2];
+            phase_b<MODE, RSM>(a, sm, scratch, k, t, b, cb0, cb1, more);
+          }
     }
     __syncthreads();
     if (tid < nk) {
@@ -1174,7 +1213,7 @@ __global__ void __launch_bounds__(kGThreads) k_plain_b(FwdArgs a, int t) {
   for (int i = threadIdx.x; i <= a.P; i += blockDim.x) sm.ib[i] = a.ibase[i];
   __syncthreads();
   phase_b<MODE, false>(a, sm, scratch, 0, t, blockIdx.x, a.colbase[blockIdx.x],
-                       a.colbase[blockIdx.x + 1]);
+                       a.colbase[blockIdx.x + 1], false);
 }
 
 // Zero wave slot 0's global state of block b (plain path, once per sample).
