@@ -153,20 +153,24 @@ __device__ __forceinline__ void fwd_neuron(const BpArgs& a, int t, int j, float 
       my_w = RES ? we.in_w[eb + lane] : a.w[a.in_eidx[eb + lane]];
     }
     if constexpr (!SMOOTH) {
-      // the spike words of kEdgeBatch edges are loaded together, then added
-      // in edge order (the order of the sum is unchanged)
+      // each lane turns its own edge into an offset into the spike-word
+      // history and a validity bit; the spike words of kEdgeBatch edges are
+      // then loaded together and added in edge order (the order of the sum is
+      // unchanged)
+      const unsigned okm = __ballot_sync(0xffffffffu, lane < n && t - my_d >= 0);
+      size_t my_off = 0;
+      if ((okm >> lane) & 1u) my_off = ((size_t)(t - my_d) * a.N + my_pre) * KB;
       for (int q0 = 0; q0 < n; q0 += kEdgeBatch<KB>) {
         uint32_t wv[kEdgeBatch<KB>][KB];
         float wwv[kEdgeBatch<KB>];
 #pragma unroll
         for (int u = 0; u < kEdgeBatch<KB>; ++u) {
-          const int q = q0 + u;
-          const int pre = __shfl_sync(0xffffffffu, my_pre, q & 31);
-          const int d = __shfl_sync(0xffffffffu, my_d, q & 31);
-          wwv[u] = __shfl_sync(0xffffffffu, my_w, q & 31);
-          const int ts = t - d;
-          const bool ok = q < n && ts >= 0;
-          const uint32_t* wp = a.bits + ((size_t)(ok ? ts : 0) * a.N + pre) * KB;
+          const int src = (q0 + u) & 31;  // q0 + u < 32: kEdgeBatch divides 32
+          const unsigned olo = __shfl_sync(0xffffffffu, (unsigned)my_off, src);
+          const unsigned ohi = __shfl_sync(0xffffffffu, (unsigned)(my_off >> 32), src);
+          wwv[u] = __shfl_sync(0xffffffffu, my_w, src);
+          const bool ok = (okm >> src) & 1u;
+          const uint32_t* wp = a.bits + (((size_t)ohi << 32) | olo);
 #pragma unroll
           for (int k = 0; k < KB; ++k) wv[u][k] = ok ? wp[k] : 0u;
         }
