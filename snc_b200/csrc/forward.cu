@@ -98,6 +98,7 @@ struct FwdArgs {
   float* elig;
   unsigned long long* fires;
   float gamma, trace_decay;
+  int s_table;  // tier S SORT: shared memory holds the whole-chunk cell table
   // deferred eligibility: psi of every ring column and step, [B][ncols][psi_T]
   // (null: eligibility accumulated in the forward into elig)
   float* psi_hist;
@@ -105,10 +106,16 @@ struct FwdArgs {
 };
 
 // Shared-memory bytes of the tier-S kernel for this graph.
-static size_t tier_s_bytes(int N, int ncols, int R, int noc, int mode, bool eprop, int nthr) {
+// Tier S SORT may add a per-cell table for whole chunks: kSTable keys, as
+// many list heads and one link per staged event.
+constexpr int kSTable = 2048;
+
+static size_t tier_s_bytes(int N, int ncols, int R, int noc, int mode, bool eprop, int nthr,
+                           bool table = false) {
   size_t words = (size_t)R * ncols + 4 * (size_t)N + (size_t)noc;
   if (mode == MODE_SORT) words += (size_t)N + 1 + 2 * (size_t)ncols + 4 * (size_t)nthr;
   if (eprop) words += (size_t)N + ncols;
+  if (mode == MODE_SORT && table) words += 2 * (size_t)kSTable + nthr;
   return words * 4 + 16;
 }
 
@@ -180,13 +187,13 @@ static_assert(kCellTable + kCountMax <= kGChunk, "the links live in st_col beyon
 
 // Table sizes (keys; as many list heads follow) and their hash bits.
 template <int TS>
-constexpr int kTabBits = TS == 1024 ? 10 : 9;
+constexpr int kTabBits = TS == 2048 ? 11 : (TS == 1024 ? 10 : 9);
 
 // Enters staged event q of cell (c, sl) into a table of TS keys (at most TS / 2
 // distinct cells); returns its entry.
 template <int TS>
 __device__ __forceinline__ unsigned cell_insert(int* tab, int* link, int q, int c, int sl, bool* first) {
-  static_assert(TS == 512 || TS == 1024, "table size");
+  static_assert(TS == 512 || TS == 1024 || TS == 2048, "table size");
   unsigned* key = reinterpret_cast<unsigned*>(tab);
   const unsigned k = (unsigned)c * 256u + (unsigned)sl + 1u;  // slot < 256, 0 = empty
   unsigned h = (k * 2654435761u) >> (32 - kTabBits<TS>);
@@ -424,6 +431,9 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
   float* tr = MODE == MODE_SORT ? reinterpret_cast<float*>(st_next + CH)
                                 : reinterpret_cast<float*>(counts + noc);
   float* psi = tr + N;
+  // SORT with a.s_table: the per-cell table for whole chunks (kSTable keys,
+  // kSTable list heads, CH links)
+  int* ctab = reinterpret_cast<int*>(EP ? psi + nc : tr);
 
   for (;;) {
     if (tid == 0) s_q = (int)atomicAdd(&a.ctl[1], 1u);
@@ -551,6 +561,34 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
         }
         __syncthreads();
         const int E = base;
+        if (a.s_table) {
+          // per-cell apply of whole chunks (CH = blockDim.x: thread q stages
+          // event q of the chunk and enters it in its cell's list; staging
+          // order is the (pre, edge) order)
+          for (int e0 = 0; e0 < E; e0 += CH) {
+            const int ce = min(CH, E - e0);
+            for (int i = tid; i < 2 * kSTable; i += nthr) ctab[i] = 0;
+            __syncthreads();
+            const int q = tid;
+            int c = 0, sl = 0;
+            unsigned h = 0;
+            bool first = false;
+            if (q < ce) {
+              const int e = e0 + q;
+              const int k = upper_index(pref, nf, e);
+              const uint2 ed = a.edges[fired[k] + (e - pref[k])];
+              sl = ring_slot(s0, edge_delay(ed), R);
+              c = edge_col(ed);
+              st_w[q] = edge_w(ed);
+              h = cell_insert<kSTable>(ctab, ctab + 2 * kSTable, q, c, sl, &first);
+            }
+            __syncthreads();
+            if (first)
+              cell_apply<false, false, kSTable>(ctab, ctab + 2 * kSTable, nullptr, st_w, h, q, c, sl, ring,
+                                                nc, 0);
+            __syncthreads();
+          }
+        } else
         for (int e0 = 0; e0 < E; e0 += CH) {
           const int ce = min(CH, E - e0);
           for (int qq = tid; qq < ce; qq += nthr) {
@@ -1301,12 +1339,31 @@ static int optin_smem() {
 }
 
 template <int MODE, bool EP>
-static int launch_tier_s_kernel(const Graph* g, int B, const FwdArgs& a, cudaStream_t st) {
+static int launch_tier_s_kernel(const Graph* g, int B, const FwdArgs& a_in, cudaStream_t st) {
   const int nthr = 1024;
-  const size_t smem = tier_s_bytes(g->N, g->ncols, g->R, a.noc, MODE, EP, nthr);
+  FwdArgs a = a_in;
+  size_t smem = tier_s_bytes(g->N, g->ncols, g->R, a.noc, MODE, EP, nthr);
   SNCB_CUDA(cudaFuncSetAttribute(k_tier_s<MODE, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   SNCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tier_s<MODE, EP>, nthr, smem));
+  a.s_table = 0;
+  if (MODE == MODE_SORT) {
+    // the per-cell table when it fits without costing a CTA per SM
+    const size_t smem_t = tier_s_bytes(g->N, g->ncols, g->R, a.noc, MODE, EP, nthr, true);
+    int per_sm_t = 0;
+    if ((int)smem_t <= optin_smem() &&
+        cudaFuncSetAttribute(k_tier_s<MODE, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t) ==
+            cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, k_tier_s<MODE, EP>, nthr, smem_t) ==
+            cudaSuccess &&
+        per_sm_t >= per_sm && per_sm_t >= 1) {
+      smem = smem_t;
+      a.s_table = 1;
+    } else {
+      cudaGetLastError();
+      SNCB_CUDA(cudaFuncSetAttribute(k_tier_s<MODE, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+  }
   if (per_sm < 1) {
     set_error("tier S does not fit on an SM");
     return SNC_B200_EUNSUPPORTED;
