@@ -143,43 +143,53 @@ __device__ __forceinline__ void fwd_neuron(const BpArgs& a, int t, int j, float 
 #pragma unroll
   for (int k = 0; k < KB; ++k) acc[k] = 0.f;
   const int e0 = RES ? 0 : a.col_ptr[j], e1 = RES ? we.nin : a.col_ptr[j + 1];
-  for (int eb = e0; eb < e1; eb += 32) {
+  // one lane per incoming edge of a 32-edge group: its pre, delay, weight
+  // and (step form) the spike words of its pre at t - d
+  auto group = [&](int eb, int& pre, int& d, float& w, uint32_t (&mw)[KB]) {
     const int n = min(32, e1 - eb);
-    int my_pre = 0, my_d = 1 << 30;
-    float my_w = 0.f;
+    pre = 0;
+    d = 1 << 30;
+    w = 0.f;
     if (lane < n) {
-      my_pre = RES ? we.in_pre[eb + lane] : a.in_pre[eb + lane];
-      my_d = RES ? we.in_d[eb + lane] : a.in_d[eb + lane];
-      my_w = RES ? we.in_w[eb + lane] : a.w[a.in_eidx[eb + lane]];
+      pre = RES ? we.in_pre[eb + lane] : a.in_pre[eb + lane];
+      d = RES ? we.in_d[eb + lane] : a.in_d[eb + lane];
+      w = RES ? we.in_w[eb + lane] : a.w[a.in_eidx[eb + lane]];
     }
     if constexpr (!SMOOTH) {
-      // each lane turns its own edge into an offset into the spike-word
-      // history and a validity bit; the spike words of kEdgeBatch edges are
-      // then loaded together and added in edge order (the order of the sum is
-      // unchanged)
-      const unsigned okm = __ballot_sync(0xffffffffu, lane < n && t - my_d >= 0);
-      size_t my_off = 0;
-      if ((okm >> lane) & 1u) my_off = ((size_t)(t - my_d) * a.N + my_pre) * KB;
-      for (int q0 = 0; q0 < n; q0 += kEdgeBatch<KB>) {
-        uint32_t wv[kEdgeBatch<KB>][KB];
-        float wwv[kEdgeBatch<KB>];
+      const bool ok = lane < n && t - d >= 0;
+      const uint32_t* wp = a.bits + ((size_t)(ok ? t - d : 0) * a.N + pre) * KB;
 #pragma unroll
-        for (int u = 0; u < kEdgeBatch<KB>; ++u) {
-          const int src = (q0 + u) & 31;  // q0 + u < 32: kEdgeBatch divides 32
-          const unsigned olo = __shfl_sync(0xffffffffu, (unsigned)my_off, src);
-          const unsigned ohi = __shfl_sync(0xffffffffu, (unsigned)(my_off >> 32), src);
-          wwv[u] = __shfl_sync(0xffffffffu, my_w, src);
-          const bool ok = (okm >> src) & 1u;
-          const uint32_t* wp = a.bits + (((size_t)ohi << 32) | olo);
+      for (int k = 0; k < KB; ++k) mw[k] = ok ? wp[k] : 0u;
+    }
+  };
+  int my_pre, my_d;
+  float my_w;
+  uint32_t mw[KB];
+  if (e0 < e1) group(e0, my_pre, my_d, my_w, mw);
+  for (int eb = e0; eb < e1; eb += 32) {
+    const int n = min(32, e1 - eb);
+    if constexpr (!SMOOTH) {
+      // the next group's spike words are requested before this group's are
+      // added: the words of 64 edges are one round trip; the words are
+      // broadcast by shuffles and added in edge order (the order of the sum
+      // is unchanged)
+      int nx_pre = 0, nx_d = 0;
+      float nx_w = 0.f;
+      uint32_t nx_mw[KB];
+      if (eb + 32 < e1) group(eb + 32, nx_pre, nx_d, nx_w, nx_mw);
+      for (int q = 0; q < n; ++q) {
+        const float ww = __shfl_sync(0xffffffffu, my_w, q);
 #pragma unroll
-          for (int k = 0; k < KB; ++k) wv[u][k] = ok ? wp[k] : 0u;
+        for (int k = 0; k < KB; ++k) {
+          const uint32_t word = __shfl_sync(0xffffffffu, mw[k], q);
+          if ((word >> lane) & 1u) acc[k] = __fadd_rn(acc[k], ww);
         }
-#pragma unroll
-        for (int u = 0; u < kEdgeBatch<KB>; ++u)
-#pragma unroll
-          for (int k = 0; k < KB; ++k)
-            if ((wv[u][k] >> lane) & 1u) acc[k] = __fadd_rn(acc[k], wwv[u]);
       }
+      my_pre = nx_pre;
+      my_d = nx_d;
+      my_w = nx_w;
+#pragma unroll
+      for (int k = 0; k < KB; ++k) mw[k] = nx_mw[k];
     } else {
       for (int q = 0; q < n; ++q) {
         const int pre = __shfl_sync(0xffffffffu, my_pre, q);
@@ -194,6 +204,7 @@ __device__ __forceinline__ void fwd_neuron(const BpArgs& a, int t, int j, float 
           if (b < a.B) acc[k] = __fadd_rn(acc[k], __fmul_rn(ww, sp[b]));
         }
       }
+      if (eb + 32 < e1) group(eb + 32, my_pre, my_d, my_w, mw);
     }
   }
 #pragma unroll
