@@ -228,4 +228,27 @@ __device__ __forceinline__ int ballot_compact(int flag, int* scratch, int* total
   return pos;
 }
 
+// ballot_compact with one CTA barrier instead of three: every warp scans the
+// per-warp counts itself, and the caller alternates between two 32-int
+// buffers (a buffer is written again only two calls later, after every
+// thread has passed the barrier of the call in between).  blockDim <= 1024.
+__device__ __forceinline__ int ballot_compact_1(int flag, int* buf, int* total, unsigned* mask) {
+  const unsigned m = __ballot_sync(0xffffffffu, flag);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  if (lane == 0) buf[warp] = __popc(m);
+  __syncthreads();
+  const int c = lane < nw ? buf[lane] : 0;
+  int incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const int before = __shfl_sync(0xffffffffu, incl - c, warp);
+  *total = __shfl_sync(0xffffffffu, incl, 31);
+  *mask = m;
+  return before + __popc(m & ((1u << lane) - 1u));
+}
+
 }  // namespace sncb

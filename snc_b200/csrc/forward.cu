@@ -742,6 +742,8 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, unsigne
   uint32_t* rast = a.raster ? a.raster + a.raster_off[sample] + (size_t)t * a.W : nullptr;
   int nf = 0;
   long long my_events = 0;
+  __shared__ int s_bc[2][32];  // ballot_compact_1 buffers, alternated
+  int bcp = 0;
   for (int base = lo; base < hi; base += nthr) {
     const int j = base + tid, jj = j - lo;
     int f = 0;
@@ -789,7 +791,8 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, unsigne
     }
     int tot;
     unsigned m;
-    const int pos = ballot_compact(f, scratch, &tot, &m);
+    const int pos = ballot_compact_1(f, s_bc[bcp], &tot, &m);
+    bcp ^= 1;
     if (rast && lane == 0 && base + warp * 32 < hi) rast[(base + warp * 32) >> 5] = m;
     if (f) sm.fired[nf + pos] = j;
     nf += tot;
