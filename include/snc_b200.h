@@ -326,6 +326,13 @@ int snc_b200_bptt_set_resident(snc_b200_bptt* h, int32_t enable);
  * overlap.  Asynchronous on stream. */
 int snc_b200_leaky_scan(const float* x, float* y, int32_t T, int64_t n, float decay, int32_t reverse,
                         void* stream);
+/* Layout change between torch's [T][B][N] and the batch-innermost [T][N][B]
+ * of the BPTT kernels: out[t][i][j] = in[t * st_t + i + j * st_j] (element
+ * strides; unit stride along i), out contiguous [T][I][J]; T <= 65535.
+ * Data movement only.  Asynchronous on stream.  No reference counterpart (the
+ * reference bridge keeps torch's layout). */
+int snc_b200_transpose(const float* in, float* out, int32_t T, int32_t I, int32_t J, int64_t st_t,
+                       int64_t st_j, void* stream);
 
 /* The BPTT forward for callers that must not allocate device memory when
  * they call it (no counterpart in the reference, which allocates inside every

@@ -91,6 +91,7 @@ SIGNATURES = {
     "snc_b200_bptt_backward": (C.c_int, [P, P, P, I32, I32, C.c_float, C.c_float, C.c_float, I32,
                                          I32, P, P, P, P, P, P, P]),
     "snc_b200_leaky_scan": (C.c_int, [P, P, I32, C.c_int64, C.c_float, I32, P]),
+    "snc_b200_transpose": (C.c_int, [P, P, I32, I32, I32, C.c_int64, C.c_int64, P]),
     "snc_b200_bptt_forward_static": (C.c_int, [P, P, P, I32, I32, C.c_float, C.c_float, C.c_float,
                                                I32, I32, P, P, P, P]),
 }

@@ -94,6 +94,30 @@ class SpikingCore:
             self.release()
 
 
+def _transpose(x, I, J, st_t, st_j, T):
+    out = torch.empty(T, I, J, device=x.device, dtype=torch.float32)
+    check(lib().snc_b200_transpose(_ptr(x), _ptr(out), T, I, J, st_t, st_j, _stream()), "transpose")
+    return out
+
+
+def _to_tnb(x):
+    """[T, B, N] fp32 (a view with unit stride along N is read in place) ->
+    contiguous [T, N, B], the kernels' batch-innermost layout."""
+    T, B, N = x.shape
+    x = x.float()
+    if x.stride(2) != 1 or T > 65535:
+        return x.permute(0, 2, 1).contiguous()
+    return _transpose(x, N, B, x.stride(0), x.stride(1), T)
+
+
+def _from_tnb(y):
+    """Contiguous [T, N, B] -> contiguous [T, B, N]."""
+    T, N, B = y.shape
+    if T > 65535:
+        return y.permute(0, 2, 1).contiguous()
+    return _transpose(y, B, N, N * B, B, T)
+
+
 class SNNFunction(torch.autograd.Function):
     """spikes [T, B, N] = core(w [S], ext [T, B, N]); fp32 CUDA tensors."""
 
@@ -103,7 +127,7 @@ class SNNFunction(torch.autograd.Function):
         if N != core.N:
             raise ValueError("ext has the wrong number of neurons")
         check(lib().snc_b200_set_device(ext.device.index or 0), "set_device")
-        ext_t = ext.detach().permute(0, 2, 1).contiguous()
+        ext_t = _to_tnb(ext.detach())
         w_csr = core.to_csr(w.detach()).contiguous()
         KB = (B + 31) // 32
         dev = ext.device
@@ -117,7 +141,7 @@ class SNNFunction(torch.autograd.Function):
               "bptt_forward")
         ctx.core, ctx.args = core, (T, B, float(threshold), float(decay), float(slope), K, int(bool(smooth)))
         ctx.save_for_backward(w_csr, ext_t, spikes, bits, vsaved)
-        return spikes.permute(0, 2, 1)
+        return _from_tnb(spikes)
 
     @staticmethod
     def backward(ctx, g_spikes):
@@ -125,7 +149,7 @@ class SNNFunction(torch.autograd.Function):
         core = ctx.core
         T, B, thr, decay, slope, K, smooth = ctx.args
         check(lib().snc_b200_set_device(ext_t.device.index or 0), "set_device")
-        g_t = g_spikes.permute(0, 2, 1).contiguous().float()
+        g_t = _to_tnb(g_spikes)
         grad_w = torch.empty(core.S, device=ext_t.device, dtype=torch.float32)
         want_ext = ctx.needs_input_grad[1]
         grad_ext = torch.empty_like(ext_t) if want_ext else None
@@ -134,7 +158,7 @@ class SNNFunction(torch.autograd.Function):
                                            _ptr(g_t), _ptr(grad_w), _ptr(grad_ext), _stream()),
               "bptt_backward")
         gw = core.from_csr(grad_w) if ctx.needs_input_grad[0] else None
-        ge = grad_ext.permute(0, 2, 1) if want_ext else None
+        ge = _from_tnb(grad_ext) if want_ext else None
         return gw, ge, None, None, None, None, None, None
 
 

@@ -590,6 +590,28 @@ __global__ void k_leaky_scan(const float* __restrict__ x, float* __restrict__ y,
   }
 }
 
+// out[t][i][j] = in[t * st_t + i + j * st_j]: the batch-innermost layout of
+// the BPTT kernels and torch's [T][B][N] (or a view of it with unit stride
+// along N) into each other, through 32 x 32 shared-memory tiles so that both
+// the reads (along i) and the writes (along j) are coalesced.
+__global__ void k_transpose_tile(const float* __restrict__ in, float* __restrict__ out, int I, int J,
+                                 long long st_t, long long st_j) {
+  __shared__ float tile[32][33];
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  const long long t = blockIdx.z;
+  const float* src = in + t * st_t;
+  float* dst = out + t * (long long)I * J;
+  for (int jj = threadIdx.y; jj < 32; jj += 8) {
+    const int i = i0 + threadIdx.x, j = j0 + jj;
+    if (i < I && j < J) tile[jj][threadIdx.x] = src[i + (long long)j * st_j];
+  }
+  __syncthreads();
+  for (int ii = threadIdx.y; ii < 32; ii += 8) {
+    const int j = j0 + threadIdx.x, i = i0 + ii;
+    if (i < I && j < J) dst[(long long)i * J + j] = tile[threadIdx.x][ii];
+  }
+}
+
 extern "C" {
 
 int snc_b200_bptt_create(int32_t N, int32_t S, const int32_t* row_ptr, const int32_t* post,
@@ -737,6 +759,18 @@ int snc_b200_leaky_scan(const float* x, float* y, int32_t T, int64_t n, float de
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int grid = (int)std::max(1ll, std::min<long long>(((long long)n + 255) / 256, (long long)sms * 16));
   k_leaky_scan<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(x, y, T, n, decay, reverse ? 1 : 0);
+  SNCB_CUDA(cudaGetLastError());
+  return SNC_B200_OK;
+}
+
+int snc_b200_transpose(const float* in, float* out, int32_t T, int32_t I, int32_t J, int64_t st_t,
+                       int64_t st_j, void* stream) {
+  if (T < 0 || I < 0 || J < 0 || T > 65535) { set_error("transpose: bad size"); return SNC_B200_EINVAL; }
+  if ((long long)T * I * J == 0) return SNC_B200_OK;
+  if (!in || !out) { set_error("transpose: null tensor"); return SNC_B200_EINVAL; }
+  const dim3 grid((unsigned)((I + 31) / 32), (unsigned)((J + 31) / 32), (unsigned)T);
+  if (grid.y > 65535) { set_error("transpose: J too large"); return SNC_B200_EINVAL; }
+  k_transpose_tile<<<grid, dim3(32, 8), 0, static_cast<cudaStream_t>(stream)>>>(in, out, I, J, st_t, st_j);
   SNCB_CUDA(cudaGetLastError());
   return SNC_B200_OK;
 }

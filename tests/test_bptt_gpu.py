@@ -260,3 +260,15 @@ def test_hub_neuron_beyond_the_resident_limit():
     np.testing.assert_array_equal(s.numpy(), rs.numpy())
     rel_close(gw, rgw)
     rel_close(ge, rge)
+
+
+def test_layout_transpose_matches_torch():
+    # the tiled layout change around the kernels, on a contiguous tensor, a
+    # [B, T, N] tensor seen as [T, B, N], and ragged tile edges
+    gen = torch.Generator().manual_seed(11)
+    x = torch.randn(7, 45, 70, generator=gen).to(DEV)
+    np.testing.assert_array_equal(BP._to_tnb(x).cpu().numpy(), x.permute(0, 2, 1).contiguous().cpu().numpy())
+    y = torch.randn(45, 7, 70, generator=gen).to(DEV).transpose(0, 1)
+    np.testing.assert_array_equal(BP._to_tnb(y).cpu().numpy(), y.permute(0, 2, 1).contiguous().cpu().numpy())
+    z = torch.randn(5, 33, 129, generator=gen).to(DEV)
+    np.testing.assert_array_equal(BP._from_tnb(z).cpu().numpy(), z.permute(0, 2, 1).contiguous().cpu().numpy())
