@@ -434,6 +434,8 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
   // SORT with a.s_table: the per-cell table for whole chunks (kSTable keys,
   // kSTable list heads, CH links)
   int* ctab = reinterpret_cast<int*>(EP ? psi + nc : tr);
+  if (MODE == MODE_SORT && a.s_table)
+    for (int i = tid; i < 2 * kSTable; i += nthr) ctab[i] = 0;  // ordered by the loop's first barrier
 
   for (;;) {
     if (tid == 0) s_q = (int)atomicAdd(&a.ctl[1], 1u);
@@ -565,10 +567,10 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
           // per-cell apply of whole chunks (CH = blockDim.x: thread q stages
           // event q of the chunk and enters it in its cell's list; staging
           // order is the (pre, edge) order)
+          // the table is all zero between chunks: every cell's owner clears
+          // its entry once it has applied the cell (nobody else reads it)
           for (int e0 = 0; e0 < E; e0 += CH) {
             const int ce = min(CH, E - e0);
-            for (int i = tid; i < 2 * kSTable; i += nthr) ctab[i] = 0;
-            __syncthreads();
             const int q = tid;
             int c = 0, sl = 0;
             unsigned h = 0;
@@ -583,9 +585,12 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
               h = cell_insert<kSTable>(ctab, ctab + 2 * kSTable, q, c, sl, &first);
             }
             __syncthreads();
-            if (first)
+            if (first) {
               cell_apply<false, false, kSTable>(ctab, ctab + 2 * kSTable, nullptr, st_w, h, q, c, sl, ring,
                                                 nc, 0);
+              ctab[h] = 0;
+              ctab[kSTable + h] = 0;
+            }
             __syncthreads();
           }
         } else
