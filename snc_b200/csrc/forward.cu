@@ -789,6 +789,13 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, unsigne
       }
       if (f) {
         my_events += PERSIST ? sm.rp[jj + 1] - sm.rp[jj] : a.row_ptr[j + 1] - a.row_ptr[j];
+        if (MODE != MODE_ATOMIC && PERSIST) {
+          // the row's groups are read again when this step's descriptors are
+          // posted: start bringing them into L1 while the fired list is built
+          const int2* gr = a.groups + sm.gp[jj];
+          asm volatile("prefetch.global.L1 [%0];" ::"l"(gr));
+          asm volatile("prefetch.global.L1 [%0];" ::"l"(a.groups + max(sm.gp[jj], sm.gp[jj + 1] - 1)));
+        }
         const int oc = PERSIST ? sm.och[jj] : a.out_ch[j];
         if (oc >= 0) atomicAdd(&a.counts[(size_t)sample * a.noc + oc], 1);
         if (EPR && a.fires) atomicAdd(&a.fires[j], 1ull);
