@@ -120,7 +120,7 @@ __device__ __forceinline__ bool grid_sync(unsigned* ctr, unsigned target, int* e
     int ok = 1;
     unsigned long long t0 = 0;
     unsigned spins = 0;
-    while (ld_relaxed_u32(ctr) < target) {
+    while (ld_acquire_u32(ctr) < target) {
       if ((++spins & 255u) == 0) {
         if (ld_volatile_i32(err) != 0) { ok = 0; break; }
         const unsigned long long now = global_ns();
@@ -132,8 +132,7 @@ __device__ __forceinline__ bool grid_sync(unsigned* ctr, unsigned target, int* e
         }
       }
     }
-    fence_acq_rel_gpu();  // acquire: later reads see the other CTAs' writes
-    s_ok = ok;
+    s_ok = ok;  // the acquire load orders later reads after the other CTAs' writes
   }
   __syncthreads();
   return s_ok != 0;
@@ -153,7 +152,7 @@ __device__ __forceinline__ bool grid_wait(unsigned* ctr, unsigned target, int* e
     int ok = 1;
     unsigned long long t0 = 0;
     unsigned spins = 0;
-    while (ld_relaxed_u32(ctr) < target) {
+    while (ld_acquire_u32(ctr) < target) {
       if ((++spins & 255u) == 0) {
         if (ld_volatile_i32(err) != 0) { ok = 0; break; }
         const unsigned long long now = global_ns();
@@ -165,8 +164,7 @@ __device__ __forceinline__ bool grid_wait(unsigned* ctr, unsigned target, int* e
         }
       }
     }
-    fence_acq_rel_gpu();
-    s_ok = ok;
+    s_ok = ok;  // the acquire load orders later reads after the other CTAs' writes
   }
   __syncthreads();
   return s_ok != 0;
