@@ -569,22 +569,28 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
           // order is the (pre, edge) order)
           // the table is all zero between chunks: every cell's owner clears
           // its entry once it has applied the cell (nobody else reads it)
+          // thread q's edge of the next chunk is requested before this
+          // chunk's cells are applied, so the load overlaps the apply
+          const int q = tid;
+          auto edge_of = [&](int e) {
+            const int k = upper_index(pref, nf, e);
+            return a.edges[fired[k] + (e - pref[k])];
+          };
+          uint2 ed_next = q < E ? edge_of(q) : make_uint2(0u, 0u);
           for (int e0 = 0; e0 < E; e0 += CH) {
             const int ce = min(CH, E - e0);
-            const int q = tid;
+            const uint2 ed = ed_next;
             int c = 0, sl = 0;
             unsigned h = 0;
             bool first = false;
             if (q < ce) {
-              const int e = e0 + q;
-              const int k = upper_index(pref, nf, e);
-              const uint2 ed = a.edges[fired[k] + (e - pref[k])];
               sl = ring_slot(s0, edge_delay(ed), R);
               c = edge_col(ed);
               st_w[q] = edge_w(ed);
               h = cell_insert<kSTable>(ctab, ctab + 2 * kSTable, q, c, sl, &first);
             }
             __syncthreads();
+            if (e0 + CH + q < E) ed_next = edge_of(e0 + CH + q);
             if (first) {
               cell_apply<false, false, kSTable>(ctab, ctab + 2 * kSTable, nullptr, st_w, h, q, c, sl, ring,
                                                 nc, 0);
