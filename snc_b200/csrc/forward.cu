@@ -816,8 +816,12 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, unsigne
     nf += tot;
   }
   __syncthreads();
-  int* fo = a.fired + ((size_t)k * 2 + par) * N + lo;
-  for (int i = tid; i < nf; i += nthr) __stcg(&fo[i], sm.fired[i]);
+  if (MODE == MODE_SORT) {
+    // the ascending fired list, for phase_b_scan (SORT steps whose inbox
+    // overflows); the other modes never read it
+    int* fo = a.fired + ((size_t)k * 2 + par) * N + lo;
+    for (int i = tid; i < nf; i += nthr) __stcg(&fo[i], sm.fired[i]);
+  }
   {
     unsigned long long wev = (unsigned long long)my_events;
 #pragma unroll
@@ -825,7 +829,7 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, unsigne
     if (lane == 0 && wev) atomicAdd(acc ? &acc[kMaxWave + k] : &a.events[sample], wev);
   }
   if (tid == 0) {
-    __stcg(&a.fired_cnt[((size_t)k * 2 + par) * P + b], nf);
+    if (MODE == MODE_SORT) __stcg(&a.fired_cnt[((size_t)k * 2 + par) * P + b], nf);
     if (nf) atomicAdd(acc ? &acc[k] : &a.spikes[sample], (unsigned long long)nf);
   }
   if (MODE == MODE_ATOMIC) {
