@@ -30,9 +30,10 @@
 //           descriptor per destination block to that block's inbox; after the
 //           barrier each block expands its inbox and accumulates into its
 //           shared-memory ring slice with shared atomics.
-//   SORT    as BUCKET, but the inbox is sorted by first edge and every ring
-//           cell receives its contributions in (pre, edge) order: the result
-//           is bit-identical to the serial CPU backend.
+//   SORT    as BUCKET, but every ring cell receives its contributions in
+//           (pre, edge) order -- per-cell lists in a shared hash table, each
+//           ordered by gedges index or staging order: the result is
+//           bit-identical to the serial CPU backend.
 #include <algorithm>
 #include <climits>
 #include <cstring>
