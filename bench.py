@@ -194,7 +194,35 @@ def cpu_baseline(g, ev, lif, budget_s=10.0):
         e += r["events"]
         n += 1
     return {"value": e / t, "unit": UNIT, "cores": 1, "kind": kind,
-            "sample": f"{n} full rec100k forwards (1000 steps, batch 1), serial cpu backend"}
+            "sample": f"{n} full rec100k forwards (1000 steps, batch 1), serial cpu backend"}, r
+
+
+def parity_leg(dg, di, g, ev, lif, timed_mode, timed_out, ref_counts):
+    """Results of the timed input checked against the CPU: the SORT mode's
+    rasters, final potentials, logits and counts against the restatement
+    (oracle), its counts and logits against the reference's own serial
+    backend run by cpu_baseline on the same input, and the timed mode's
+    spike and event totals against the reference's."""
+    from oracle import oracle as O
+    from snc_b200 import runtime as R
+    run = R.Run(dg, di, raster=True, vfinal=True, cuda_graph=True)
+    run.launch(lif, mode=R.MODE_SORT, path=R.PATH_PERSISTENT)
+    o = run.fetch(raster=True, vfinal=True)
+    run.release()
+    ref = O.forward_batched(g, ev, np.array([1000], np.int32), lif)
+    exact = all(np.array_equal(o[k], ref[k]) for k in ("spikes", "events", "logits", "raster")) and \
+        np.array_equal(o["v"].view(np.uint32), ref["v"].view(np.uint32))
+    out = {"input": "the timed rec100k input (seed 1)", "sort_exact_vs_oracle": bool(exact)}
+    if ref_counts is not None:
+        out["sort_counts_equal_reference"] = bool(
+            int(o["spikes"][0]) == ref_counts["spikes"] and int(o["events"][0]) == ref_counts["events"]
+            and np.array_equal(o["logits"][0], ref_counts["logits"]))
+        rs, re_ = float(ref_counts["spikes"]), float(ref_counts["events"])
+        ts, te = float(timed_out["total_spikes"]), float(timed_out["total_events"])
+        name = R.MODE_NAMES[timed_mode]
+        out[f"{name}_spike_agreement"] = min(ts, rs) / max(ts, rs, 1.0)
+        out[f"{name}_event_agreement"] = min(te, re_) / max(te, re_, 1.0)
+    return out
 
 
 def _time_cuda(fn, steps, warmup):
@@ -232,7 +260,7 @@ def config_legs(reps=3):
                                  ("C3_audio700", W.audio700_graph(), W.audio700_inputs(256))):
         dg = R.DeviceGraph(g)
         di = R.DeviceInputs(dg, ev, steps)
-        run = R.Run(dg, di)
+        run = R.Run(dg, di, cuda_graph=True)  # the persistent launch goes through a CUDA graph
         ss = int(np.sum(steps))
         leg = {"samples": int(len(steps)), "sample_steps": ss}
         for m in (R.MODE_ATOMIC, R.MODE_SORT):
@@ -245,7 +273,8 @@ def config_legs(reps=3):
                 best = min(ms[1:])
                 leg[f"{R.MODE_NAMES[m]}_{R.PATH_NAMES[p]}"] = {
                     "ms": best, "events_per_s": o["total_events"] / (best / 1e3),
-                    "sample_steps_per_s": ss / (best / 1e3)}
+                    "sample_steps_per_s": ss / (best / 1e3),
+                    "cuda_graph": bool(run.used_graph())}
         leg["persistent_vs_plain_sort"] = leg["sort_plain"]["ms"] / leg["sort_persistent"]["ms"]
         out[name] = leg
         run.release()
@@ -448,6 +477,8 @@ def our_arm(args):
     run = R.Run(dg, di, cuda_graph=True)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
+    last = {}
+
     def timed(run_, mode_, path_, k):
         ms, ev_n, sp_n = [], 0, 0
         for _ in range(k):
@@ -457,6 +488,7 @@ def our_arm(args):
             ms.append(o["ms"])
             ev_n += o["total_events"]
             sp_n += o["total_spikes"]
+            last["o"] = o
         return ms, ev_n, sp_n
 
     timed(run, mode, R.PATH_PERSISTENT, args.warmup)
@@ -469,6 +501,7 @@ def our_arm(args):
     ms, ev_n, sp_n = timed(run, mode, R.PATH_PERSISTENT, args.steps)
     torch.cuda.synchronize()
     clk = clocks.stop()
+    timed_out = last["o"]
     used_graph = run.used_graph()
     tot_ms = float(sum(ms))
     if dist:
@@ -499,7 +532,9 @@ def our_arm(args):
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         e2e_t, e2e_ev = float(mx[0]), float(t[1])
     e2e = {"value": e2e_ev / e2e_t, "unit": UNIT, "h2d_bytes_per_step": int(di.device_bytes),
-           "d2h_bytes_per_step": int(4 * max(1, dg.n_out) + 16 + 4)}
+           "d2h_bytes_per_step": int(4 * max(1, dg.n_out) + 16 + 4),
+           "graph": "resident (uploaded once before the timed region; events, schedule build, "
+                    "run and results inside it)"}
 
     extra = {}
     if not args.no_extra:
@@ -532,7 +567,9 @@ def our_arm(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_extra:
-        cpu = cpu_baseline(g, ev, lif)
+        cpu, ref_counts = cpu_baseline(g, ev, lif)
+        extra["parity"] = parity_leg(dg, di, g, ev, lif, mode, timed_out,
+                                     ref_counts if cpu["kind"] == "reference" else None)
         extra["configs"] = config_legs()
         extra["bptt"] = bptt_leg()
 

@@ -13,7 +13,6 @@
  *   snc::forward + Backend names                include/snc/runtime.hpp:21-31,57-58
  *   snc::cudatrain::*                           include/snc/cuda_trainer.hpp:26-57
  *   python/snc SNN / SurrogateSpike (BPTT)      python/snc/model.py:17-72
- * INTEGRATION.md shows the bindings a maintainer adds on the reference side.
  */
 #ifndef SNC_B200_H_
 #define SNC_B200_H_
@@ -38,7 +37,7 @@ typedef enum {
   SNC_B200_EOVERFLOW = -7     /* a device work buffer overflowed */
 } snc_b200_status;
 
-/* Read-only view of a reference SNNGraph (include/snc/snn_graph.hpp:114-148):
+/* Read-only view of a reference SNNGraph (include/snc/snn_graph.hpp:43-77):
  * CSR over OUTGOING synapses, edges in insertion order within each row.
  * branch_ids is informational in the reference and not needed here. */
 typedef struct {
@@ -53,7 +52,7 @@ typedef struct {
   const int32_t* channel;  /* [N] input feature / output class, -1 otherwise */
 } snc_graph_view;
 
-/* InputEvent (include/snc/encoders.hpp:224-229), same 16-byte layout. */
+/* InputEvent (include/snc/encoders.hpp:21-26), same 16-byte layout. */
 typedef struct {
   int32_t sample_id;
   int32_t channel_id;
@@ -118,6 +117,30 @@ int snc_b200_set_device(int device);
 /* Text of the last error on this host thread ("" if none). */
 const char* snc_b200_last_error(void);
 
+/* ---- failure detection ---------------------------------------------------
+ * No reference counterpart: the reference's GPU path has no device-side
+ * waits and reports failure only by cuda::forward returning false
+ * (src/runtime/cpu_backend.cpp:197-205).
+ *
+ * Wall-clock bound of every device-side spin wait (the grid barriers of the
+ * all-SM forward and of the BPTT kernels) for launches made from now on, in
+ * nanoseconds; 0 restores the default of 2 s.  A wait that runs out makes
+ * every block of the launch return, and the call reports SNC_B200_ETIMEOUT;
+ * the context stays usable.  Process-wide. */
+int snc_b200_set_wait_limit(uint64_t ns);
+/* Test hook: the next `n` launches that contain grid barriers (all-SM
+ * forward, BPTT forward / backward) wait at their barriers for one arrival
+ * that no block makes, so every such wait runs out after the wait limit and
+ * the launch reports SNC_B200_ETIMEOUT.  Nothing faults; the next launch
+ * without a pending stall runs normally.  Process-wide. */
+int snc_b200_inject_stall(int32_t n);
+/* Test hook: allow `after` more device allocations of this library, then
+ * fail every further one with SNC_B200_ENOMEM (after < 0: never fail).  The
+ * environment variable SNC_B200_FAIL_ALLOC sets the initial value, so a
+ * process that cannot call this (the reference's CLIs linked with the
+ * adapter) can still be made to take its CPU fallback.  Process-wide. */
+int snc_b200_inject_alloc_failure(int64_t after);
+
 /* ---- graph ----------------------------------------------------------------*/
 
 /* Validate (as SNNGraph::validate, src/graph/snn_graph.cpp:30-56) and upload a
@@ -148,7 +171,7 @@ int snc_b200_inputs_upload(const snc_b200_graph* g, const snc_input_event* event
                            snc_b200_inputs** out);
 int snc_b200_inputs_release(snc_b200_inputs* in);
 
-/* Input encoders (include/snc/encoders.hpp:14-50, src/training/encoders.cpp:25-71)
+/* Input encoders (include/snc/encoders.hpp:21-45, src/training/encoders.cpp:25-71)
  * run on the device: the schedule of a batch built straight from its
  * features [num_samples][n_channels] (host, row-major), sample b spanning
  * steps[b] steps; only the features and step counts are copied.  Encoders as
@@ -334,20 +357,23 @@ int snc_b200_leaky_scan(const float* x, float* y, int32_t T, int64_t n, float de
 int snc_b200_transpose(const float* in, float* out, int32_t T, int32_t I, int32_t J, int64_t st_t,
                        int64_t st_j, void* stream);
 
-/* The BPTT forward for callers that must not allocate device memory when
- * they call it (no counterpart in the reference, which allocates inside every
- * GPU call): a stream being captured under a mode that forbids allocation, a
- * framework whose allocator owns all device memory, a real-time loop.  Same
- * arguments and results as snc_b200_bptt_forward; the caller still provides
- * every input and output buffer, and the call makes no cudaMalloc / cudaFree.
+/* The BPTT forward for callers that cannot allocate device memory when they
+ * call it (no counterpart in the reference, which allocates inside every GPU
+ * call): a framework whose caching allocator owns all of the device's memory,
+ * so that an allocation behind its back can fail or starve it, and a
+ * real-time loop that must not pay cudaMalloc's latency or risk its failure
+ * mid-run.  Same arguments, launch and results as snc_b200_bptt_forward; the
+ * caller still provides every input and output buffer, and the call makes no
+ * cudaMalloc / cudaFree.  Like snc_b200_bptt_forward it returns after reading
+ * the kernel's error word back and waiting for `stream`.
  * Its scratch -- the membrane state of num_neurons x B samples and the
  * barrier / error words -- is one static 4 MiB array per device that every
  * device loading the library keeps until exit, so num_neurons * B must not
  * exceed 1,048,512 (SNC_B200_EUNSUPPORTED otherwise).  All calls share that
  * array: calls whose work overlaps on the GPU (different streams, threads or
  * handles without ordering) race and must not be issued.  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture. */
+ * device looks up the array's device address (cudaGetSymbolAddress) and
+ * caches it; make that first call before any stream capture. */
 int snc_b200_bptt_forward_static(snc_b200_bptt* h, const float* w, const float* ext, int32_t T,
                                  int32_t B, float threshold, float decay, float slope,
                                  int32_t ckpt_every, int32_t smooth, float* spikes,

@@ -1,1 +1,6 @@
-"""CPU checkers for the snc_b200 backend (test infrastructure only)."""
+"""CPU checkers (test infrastructure only): the restatement of the reference's
+hot path and, where the reference tree is present, the unchanged reference
+built from its sources.  SNC_REF names that tree (default /root/reference)."""
+import os
+
+REF_ROOT = os.environ.get("SNC_REF", "/root/reference")

@@ -60,7 +60,7 @@ def core_forward(w, ext, pre, post, delays, thr, decay, k, smooth=False):
 
 
 def leaky_readout(spikes, w_ro, b_ro, ro_ids, ro_decay):
-    """SHDNet's leaky readout (shd_model.py:235-236,244): out = ro_decay * out
+    """SHDNet's leaky readout (shd_model.py:139-140,147): out = ro_decay * out
     + Linear(s_top); logits = out / T after the last step."""
     T = spikes.shape[0]
     out = torch.zeros(spikes.shape[1], w_ro.shape[0], dtype=spikes.dtype, device=spikes.device)

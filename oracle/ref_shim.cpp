@@ -10,8 +10,8 @@
 // Every function here only marshals plain arrays into the reference's types
 // and calls the reference API:
 //   snc::forward               include/snc/runtime.hpp:57-58
-//   snc::encode                include/snc/encoders.hpp:45-48
-//   snc::make_static_snc etc.  include/snc/snn_graph.hpp:181-201
+//   snc::encode                include/snc/encoders.hpp:42-45
+//   snc::make_static_snc etc.  include/snc/snn_graph.hpp:118-132
 //   snc::make_synthetic        include/snc/dataset.hpp:27
 //   snc::Trainer               include/snc/trainer.hpp:59-107
 #include <cstdint>

@@ -57,6 +57,9 @@ SIGNATURES = {
     "snc_b200_inputs_encode": (C.c_int, [P, I32, P, I32, I32, P, C.c_float, C.c_float, C.c_float,
                                          C.c_uint64, P]),
     "snc_b200_last_error": (C.c_char_p, []),
+    "snc_b200_set_wait_limit": (C.c_int, [C.c_uint64]),
+    "snc_b200_inject_stall": (C.c_int, [I32]),
+    "snc_b200_inject_alloc_failure": (C.c_int, [C.c_int64]),
     "snc_b200_graph_upload": (C.c_int, [P, P]),
     "snc_b200_graph_release": (C.c_int, [P]),
     "snc_b200_graph_info": (C.c_int, [P, P, P, P, P, P]),

@@ -18,7 +18,7 @@
 // no device is usable.  Changed on purpose: the graph is uploaded once and
 // cached (the reference re-uploads per call, cuda_backend.cu:247-285);
 // minibatch inputs are host-encoded with snc::encode (same per-sample seeds
-// as the CPU Trainer, src/training/trainer.cpp:334-335,366) instead of
+// as the CPU Trainer, src/training/trainer.cpp:225-226,257) instead of
 // cuRAND draws, so every GPU run is reproducible.
 #include <algorithm>
 #include <cmath>

@@ -1,7 +1,9 @@
 // C ABI implementation: graph upload, input schedules, runs, one-call
 // forwards and the delivery autotuner.  See include/snc_b200.h.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -24,6 +26,36 @@ int cuda_fail(cudaError_t e, const char* what) {
   if (e == cudaErrorMemoryAllocation) return SNC_B200_ENOMEM;
   if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return SNC_B200_ENODEV;
   return SNC_B200_ECUDA;
+}
+
+// ---- failure injection and wait bounds ---------------------------------------
+// Device allocations left before every further one fails: -1 = never fail;
+// initialised from SNC_B200_FAIL_ALLOC (the number of allocations to allow).
+static std::atomic<long long> g_alloc_left{[] {
+  const char* e = std::getenv("SNC_B200_FAIL_ALLOC");
+  return e && *e ? std::max(-1ll, std::atoll(e)) : -1ll;
+}()};
+static std::atomic<unsigned long long> g_wait_ns{0};
+static std::atomic<int> g_stalls{0};
+
+bool alloc_fault() {
+  long long left = g_alloc_left.load();
+  while (left >= 0) {
+    if (left == 0) return true;
+    if (g_alloc_left.compare_exchange_weak(left, left - 1)) return false;
+  }
+  return false;
+}
+
+WaitCtl take_wait_ctl(bool consume) {
+  WaitCtl w{g_wait_ns.load(), 0};
+  if (consume) {
+    int n = g_stalls.load();
+    while (n > 0 && !g_stalls.compare_exchange_weak(n, n - 1)) {
+    }
+    if (n > 0) w.stall = 1;
+  }
+  return w;
 }
 
 static int check_device() {
@@ -244,7 +276,7 @@ int fetch_run(Run* r, float* logits, int64_t* spikes, int64_t* events, uint32_t*
   if (stats) {
     stats->spikes = ts;
     stats->synaptic_events = te;
-    stats->overflow = 0;
+    stats->overflow = err == SNC_B200_EOVERFLOW ? 1 : 0;
     stats->ms = ms;
   }
   if (err) {
@@ -292,6 +324,22 @@ int snc_b200_set_device(int device) {
 }
 
 const char* snc_b200_last_error(void) { return g_last_error.c_str(); }
+
+int snc_b200_set_wait_limit(uint64_t ns) {
+  g_wait_ns.store(ns);
+  return SNC_B200_OK;
+}
+
+int snc_b200_inject_stall(int32_t n) {
+  if (n < 0) { set_error("inject_stall: negative count"); return SNC_B200_EINVAL; }
+  g_stalls.store(n);
+  return SNC_B200_OK;
+}
+
+int snc_b200_inject_alloc_failure(int64_t after) {
+  g_alloc_left.store(after < 0 ? -1 : after);
+  return SNC_B200_OK;
+}
 
 int snc_b200_graph_upload(const snc_graph_view* v, snc_b200_graph** out) {
   if (!out) { set_error("null out"); return SNC_B200_EINVAL; }

@@ -65,6 +65,8 @@ struct BpArgs {
   unsigned* ctl;
   int* err;
   int res_cap;         // resident launches: edges per direction staged per warp
+  unsigned long long wait_ns;  // grid-barrier wait bound (0: the default)
+  unsigned stall;              // injected arrivals that never come (failure tests)
 };
 
 constexpr int kBpThreads = 256;
@@ -225,7 +227,7 @@ __global__ void __launch_bounds__(kBpThreads, kBpMinBlocks<KB>) k_bptt_forward(B
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int W = (gridDim.x * blockDim.x) >> 5;
   const unsigned nb = gridDim.x;
-  unsigned target = 0;
+  unsigned target = a.stall;
   WarpEdges we{};
   if (RES) {
     we = warp_edges(sm_all, a.res_cap);
@@ -262,7 +264,7 @@ __global__ void __launch_bounds__(kBpThreads, kBpMinBlocks<KB>) k_bptt_forward(B
       }
     }
     target += nb;
-    if (!grid_sync(&a.ctl[0], target, a.err)) return;
+    if (!grid_sync(&a.ctl[0], target, a.err, a.wait_ns)) return;
   }
 }
 
@@ -417,7 +419,7 @@ __global__ void __launch_bounds__(kBpThreads, kBpMinBlocks<KB>) k_bptt_backward(
   const int W = (gridDim.x * blockDim.x) >> 5;
   const unsigned nb = gridDim.x;
   const size_t NB = (size_t)a.N * a.B;
-  unsigned target = 0;
+  unsigned target = a.stall;
   WarpEdges we{};
   if (RES) {
     we = warp_edges(sm_all + (size_t)(blockDim.x >> 5) * 32 * KB, a.res_cap);
@@ -434,7 +436,7 @@ __global__ void __launch_bounds__(kBpThreads, kBpMinBlocks<KB>) k_bptt_backward(
       for (int i = gw; i < a.N; i += W)
         bwd_neuron<KB, SMOOTH, RES>(a, t, i, a.vsaved + (size_t)t * NB, sm_g, we);
       target += nb;
-      if (!grid_sync(&a.ctl[0], target, a.err)) return;
+      if (!grid_sync(&a.ctl[0], target, a.err, a.wait_ns)) return;
     }
     if (RES) flush_acc(a, we);
     return;
@@ -464,7 +466,7 @@ __global__ void __launch_bounds__(kBpThreads, kBpMinBlocks<KB>) k_bptt_backward(
       for (int i = gw; i < a.N; i += W)
         bwd_neuron<KB, SMOOTH, RES>(a, t, i, a.seg + (size_t)(t - t0) * NB, sm_g, we);
       target += nb;
-      if (!grid_sync(&a.ctl[0], target, a.err)) return;
+      if (!grid_sync(&a.ctl[0], target, a.err, a.wait_ns)) return;
     }
   }
   if (RES) flush_acc(a, we);
@@ -555,6 +557,23 @@ static int grow(T** p, size_t* cap, size_t n) {
 static int res_cap(const snc_b200_bptt* h) {
   if (!h->resident || h->max_deg > kResCapMax) return 0;
   return std::max(32, (h->max_deg + 31) / 32 * 32);
+}
+
+// Arguments of a forward launch over handle h (both forward entry points).
+static BpArgs forward_args(const snc_b200_bptt* h, const float* w, const float* ext, int T, int B,
+                           float threshold, float decay, float slope, int ckpt_every, int smooth,
+                           float* spikes, uint32_t* spike_bits, float* v_saved) {
+  BpArgs a{};
+  a.N = h->N; a.S = h->S; a.R = h->R; a.T = T; a.B = B; a.K = ckpt_every; a.smooth = smooth;
+  a.thr = threshold; a.decay = decay; a.slope = slope;
+  a.row_ptr = h->row_ptr; a.out_post = h->out_post; a.out_d = h->out_d; a.col_ptr = h->col_ptr;
+  a.in_pre = h->in_pre; a.in_d = h->in_d; a.in_eidx = h->in_eidx;
+  a.w = w; a.ext = ext; a.spikes = spikes; a.bits = spike_bits; a.vsaved = v_saved;
+  a.res_cap = res_cap(h);
+  const WaitCtl wc = take_wait_ctl(true);
+  a.wait_ns = wc.ns;
+  a.stall = wc.stall;
+  return a;
 }
 
 static int check_err(snc_b200_bptt* h, cudaStream_t st) {
@@ -701,14 +720,10 @@ int snc_b200_bptt_forward(snc_b200_bptt* h, const float* w, const float* ext, in
   const size_t NB = (size_t)h->N * B;
   int rc = grow(&h->v, &h->v_cap, NB);
   if (rc) return rc;
-  BpArgs a{};
-  a.N = h->N; a.S = h->S; a.R = h->R; a.T = T; a.B = B; a.K = ckpt_every; a.smooth = smooth;
-  a.thr = threshold; a.decay = decay; a.slope = slope;
-  a.row_ptr = h->row_ptr; a.out_post = h->out_post; a.out_d = h->out_d; a.col_ptr = h->col_ptr;
-  a.in_pre = h->in_pre; a.in_d = h->in_d; a.in_eidx = h->in_eidx;
-  a.w = w; a.ext = ext; a.spikes = spikes; a.bits = spike_bits; a.vsaved = v_saved; a.v = h->v;
+  BpArgs a = forward_args(h, w, ext, T, B, threshold, decay, slope, ckpt_every, smooth, spikes,
+                          spike_bits, v_saved);
+  a.v = h->v;
   a.ctl = h->ctl; a.err = h->err;
-  a.res_cap = res_cap(h);
   SNCB_CUDA(cudaMemsetAsync(h->ctl, 0, 16, st));
   SNCB_CUDA(cudaMemsetAsync(h->err, 0, 4, st));
   if ((rc = launch(true, smooth != 0, a, h->sm_count, st))) return rc;
@@ -742,6 +757,9 @@ int snc_b200_bptt_backward(snc_b200_bptt* h, const float* w, const float* ext, i
   a.gspk = grad_spikes; a.gw = grad_w; a.gext = grad_ext; a.gv = h->gv; a.gcur = h->gcur; a.seg = h->seg;
   a.ctl = h->ctl; a.err = h->err;
   a.res_cap = res_cap(h);
+  const WaitCtl wc = take_wait_ctl(true);
+  a.wait_ns = wc.ns;
+  a.stall = wc.stall;
   SNCB_CUDA(cudaMemsetAsync(h->ctl, 0, 16, st));
   SNCB_CUDA(cudaMemsetAsync(h->err, 0, 4, st));
   SNCB_CUDA(cudaMemsetAsync(grad_w, 0, (size_t)std::max(1, h->S) * sizeof(float), st));
@@ -781,16 +799,16 @@ int snc_b200_transpose(const float* in, float* out, int32_t T, int32_t I, int32_
 // Forward without device allocation.
 //
 // Some callers cannot allocate device memory at the moment they run the
-// forward: code executing while a stream is being captured into a CUDA graph
-// under a capture mode that forbids allocation, frameworks whose caching
-// allocator owns all device memory and treats any allocation outside it as an
-// error, and real-time loops that must not pay cudaMalloc's latency or risk
-// its failure.  snc_b200_bptt_forward may allocate on its first use at a
-// given size (the per-neuron state buffer of the handle grows on demand).
+// forward: a framework whose caching allocator owns all of the device's memory
+// (an allocation behind its back can fail or push it out of memory), and a
+// real-time loop that must not pay cudaMalloc's latency or risk its failure in
+// the middle of a run.  snc_b200_bptt_forward may allocate on its first use at
+// a given size (the per-neuron state buffer of the handle grows on demand).
 // This variant runs the same kernel with its scratch -- the membrane
 // potential of every (neuron, sample) and the barrier / error words -- in one
 // fixed array in device memory that the library reserves statically, so the
-// call itself never allocates.
+// call itself never allocates.  Like the regular forward it ends by reading
+// the kernel's error word back and waiting for `stream`.
 // ---------------------------------------------------------------------------
 namespace sncb {
 
@@ -852,12 +870,10 @@ extern "C" int snc_b200_bptt_forward_static(snc_b200_bptt* h, const float* w, co
   unsigned* ctl = static_cast<unsigned*>(base);
   int* err = reinterpret_cast<int*>(static_cast<char*>(base) + 16);
   float* v = reinterpret_cast<float*>(static_cast<char*>(base) + kStaticCtlBytes);
-  BpArgs a{};
-  a.N = h->N; a.S = h->S; a.R = h->R; a.T = T; a.B = B; a.K = ckpt_every; a.smooth = smooth;
-  a.thr = threshold; a.decay = decay; a.slope = slope;
-  a.row_ptr = h->row_ptr; a.out_post = h->out_post; a.out_d = h->out_d; a.col_ptr = h->col_ptr;
-  a.in_pre = h->in_pre; a.in_d = h->in_d; a.in_eidx = h->in_eidx;
-  a.w = w; a.ext = ext; a.spikes = spikes; a.bits = spike_bits; a.vsaved = v_saved;
+  // the same launch as snc_b200_bptt_forward (resident when the handle's
+  // degrees allow it; a resident launch needs shared memory only)
+  BpArgs a = forward_args(h, w, ext, T, B, threshold, decay, slope, ckpt_every, smooth, spikes,
+                          spike_bits, v_saved);
   a.v = v;  // zeroed by the kernel before the first step
   a.ctl = ctl;
   a.err = err;

@@ -6,8 +6,10 @@
 
 namespace sncb {
 
-// Wall-clock bound of every spin-wait in this library: a wait that has not
-// finished after this many nanoseconds sets the error word and returns.
+// Default wall-clock bound of every spin-wait in this library: a wait that
+// has not finished after this many nanoseconds sets the error word and
+// returns.  Launches carry their own bound (snc_b200_set_wait_limit); 0
+// selects this default.
 constexpr unsigned long long kSpinTimeoutNs = 2000000000ull;  // 2 s
 constexpr int kErrTimeout = -5;                               // SNC_B200_ETIMEOUT
 
@@ -95,12 +97,22 @@ __device__ __forceinline__ long long block_sum_ll(long long x, long long* scratc
   return r;
 }
 
+// Arrival count `c` has not reached `target` yet.  Counter and targets grow
+// modulo 2^32; compared by signed distance, a long launch whose count wraps
+// (about 30 M barriers of a 143-CTA grid) still waits correctly, since every
+// arrival lies within a few grids of the target being waited on.
+__device__ __forceinline__ bool before(unsigned c, unsigned target) {
+  return static_cast<int>(c - target) < 0;
+}
+
 // Software grid barrier for a cooperatively launched (co-resident) grid.
 // `ctr` counts arrivals and is never reset inside a launch; the n-th barrier
-// of the launch waits for ctr >= n * gridDim.x.  The wait is bounded: after
-// kSpinTimeoutNs it records kErrTimeout in *err and every CTA returns false,
-// so callers leave their loops and the context stays usable.
-__device__ __forceinline__ bool grid_sync(unsigned* ctr, unsigned target, int* err) {
+// of the launch waits for ctr >= n * gridDim.x (modulo 2^32, see before()).
+// The wait is bounded: after limit_ns (kSpinTimeoutNs when 0) it records
+// kErrTimeout in *err and every CTA returns false, so callers leave their
+// loops and the context stays usable.
+__device__ __forceinline__ bool grid_sync(unsigned* ctr, unsigned target, int* err,
+                                          unsigned long long limit_ns) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -110,12 +122,12 @@ __device__ __forceinline__ bool grid_sync(unsigned* ctr, unsigned target, int* e
     int ok = 1;
     unsigned long long t0 = 0;
     unsigned spins = 0;
-    while (ld_acquire_u32(ctr) < target) {
+    while (before(ld_acquire_u32(ctr), target)) {
       if ((++spins & 255u) == 0) {
         if (ld_volatile_i32(err) != 0) { ok = 0; break; }
         const unsigned long long now = global_ns();
         if (t0 == 0) t0 = now;
-        else if (now - t0 > kSpinTimeoutNs) {
+        else if (now - t0 > (limit_ns ? limit_ns : kSpinTimeoutNs)) {
           atomicCAS(err, 0, kErrTimeout);
           ok = 0;
           break;
@@ -136,18 +148,19 @@ __device__ __forceinline__ void grid_arrive(unsigned* ctr) {
   if (threadIdx.x == 0) red_release_add_u32(ctr, 1u);
 }
 
-__device__ __forceinline__ bool grid_wait(unsigned* ctr, unsigned target, int* err) {
+__device__ __forceinline__ bool grid_wait(unsigned* ctr, unsigned target, int* err,
+                                          unsigned long long limit_ns) {
   __shared__ int s_ok;
   if (threadIdx.x == 0) {
     int ok = 1;
     unsigned long long t0 = 0;
     unsigned spins = 0;
-    while (ld_acquire_u32(ctr) < target) {
+    while (before(ld_acquire_u32(ctr), target)) {
       if ((++spins & 255u) == 0) {
         if (ld_volatile_i32(err) != 0) { ok = 0; break; }
         const unsigned long long now = global_ns();
         if (t0 == 0) t0 = now;
-        else if (now - t0 > kSpinTimeoutNs) {
+        else if (now - t0 > (limit_ns ? limit_ns : kSpinTimeoutNs)) {
           atomicCAS(err, 0, kErrTimeout);
           ok = 0;
           break;

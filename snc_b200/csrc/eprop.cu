@@ -457,7 +457,7 @@ static int run_batch(snc_b200_eprop* s, const snc_input_event* ev, size_t n_ev, 
         stats->spikes += (long long)sp[b];
         stats->synaptic_events += (long long)en[b];
       }
-      stats->overflow = 0;
+      stats->overflow = err == SNC_B200_EOVERFLOW ? 1 : 0;
       stats->ms = ms;
     }
     if (ok && err) {

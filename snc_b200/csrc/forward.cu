@@ -104,6 +104,10 @@ struct FwdArgs {
   // (null: eligibility accumulated in the forward into elig)
   float* psi_hist;
   int psi_T;
+  // bound of the grid barrier's waits (0: the default) and arrivals that no
+  // block makes (a stall injected for failure tests: every wait runs out)
+  unsigned long long wait_ns;
+  unsigned stall;
 };
 
 // Shared-memory bytes of the tier-S kernel for this graph.
@@ -488,7 +492,7 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
           v[j] = vv;
           refr[j] = rr;
           if (EP) {
-            // cuda_trainer.cu:151-153: triangular surrogate and pre trace
+            // cuda_trainer.cu:93-95: triangular surrogate and pre trace
             const float thr = a.lif.thr;
             const float dd = __fdiv_rn(fabsf(__fsub_rn(vpre, thr)), thr > 0.f ? thr : 1.f);
             if (c >= 0) {
@@ -780,7 +784,7 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, unsigne
       float vpre;
       f = lif_step(a.lif, vv, rr, e, rin, EPR ? &vpre : nullptr);
       if (EPR && c >= 0) {
-        // e-prop (cuda_trainer.cu:151-152): the triangular surrogate of this
+        // e-prop (cuda_trainer.cu:93-94): the triangular surrogate of this
         // column and step, for the deferred eligibility
         const float thr = a.lif.thr;
         const float dd = __fdiv_rn(fabsf(__fsub_rn(vpre, thr)), thr > 0.f ? thr : 1.f);
@@ -1175,7 +1179,7 @@ __global__ void __launch_bounds__(kGThreadsMax, 1) k_tier_g(FwdArgs a) {
   const int lo = b * BS, hi = min(a.N, lo + BS);
   const int cb0 = a.colbase[b], cb1 = a.colbase[b + 1];
   const unsigned nb = gridDim.x;
-  unsigned target = 0;
+  unsigned target = a.stall;
   for (int jj = tid; jj < BS; jj += nthr) {
     sm.col[jj] = lo + jj < hi ? a.col_of[lo + jj] : -1;
     sm.och[jj] = lo + jj < hi ? a.out_ch[lo + jj] : -1;
@@ -1216,7 +1220,7 @@ __global__ void __launch_bounds__(kGThreadsMax, 1) k_tier_g(FwdArgs a) {
       }
     }
     target += nb;
-    if (!grid_sync(&a.ctl[0], target, a.err)) return;
+    if (!grid_sync(&a.ctl[0], target, a.err, a.wait_ns)) return;
     const int Tw = s_T[0];
     for (int t = 0; t < Tw; ++t) {
       for (int k = 0; k < nk; ++k)
@@ -1230,7 +1234,7 @@ __global__ void __launch_bounds__(kGThreadsMax, 1) k_tier_g(FwdArgs a) {
       for (int k = 0; k < nk; ++k)
         if (t + 1 < s_T[k])
           load_ext(a, sm.ext + (size_t)k * BS, s_samp[k], s_gb[k] + t + 1, t + 1, b);
-      if (!grid_wait(&a.ctl[0], target, a.err)) return;
+      if (!grid_wait(&a.ctl[0], target, a.err, a.wait_ns)) return;
       if (MODE != MODE_ATOMIC)
         for (int k = 0; k < nk; ++k)
           if (t < s_T[k]) {
@@ -1249,7 +1253,7 @@ __global__ void __launch_bounds__(kGThreadsMax, 1) k_tier_g(FwdArgs a) {
         for (int j = lo + tid; j < hi; j += nthr)
           a.vfinal[(size_t)s_samp[k] * a.N + j] = sm.v[k * BS + (j - lo)];
     target += nb;
-    if (!grid_sync(&a.ctl[0], target, a.err)) return;
+    if (!grid_sync(&a.ctl[0], target, a.err, a.wait_ns)) return;
   }
 }
 
@@ -1577,7 +1581,11 @@ int launch_run(Run* r, const snc_lif* lif, int mode, int path, cudaStream_t st) 
     }
     if ((rc = ensure_grid_state(r, Bw))) return rc;
   }
-  const FwdArgs a = make_args(r, lif);
+  FwdArgs a = make_args(r, lif);
+  const bool grid = path == SNC_B200_PATH_PERSISTENT && !use_tier_s(r, mode, path);
+  const WaitCtl wc = take_wait_ctl(grid && in->B > 0);  // only grid launches wait
+  a.wait_ns = wc.ns;
+  a.stall = wc.stall;
   const size_t B = (size_t)std::max(1, in->B);
   // The legacy default stream cannot be captured; a run owns a blocking
   // stream (ordered with the legacy stream) that stands in for it.
@@ -1597,10 +1605,12 @@ int launch_run(Run* r, const snc_lif* lif, int mode, int path, cudaStream_t st) 
   SNCB_CUDA(cudaEventRecord(r->ev0, st));
   r->used_graph = false;
   if (in->B > 0) {
+    // an injected stall is never captured: the graph keeps the normal launch
     bool use_graph = (r->flags & SNC_B200_RUN_GRAPH) && path == SNC_B200_PATH_PERSISTENT &&
-                     !r->graph_refused;
+                     !r->graph_refused && a.stall == 0;
     if (use_graph) {
       const bool same = r->gexec && r->gexec_mode == mode && r->gexec_stream == st &&
+                        r->gexec_wait_ns == a.wait_ns &&
                         std::memcmp(&r->gexec_lif, lif, sizeof(snc_lif)) == 0;
       if (!same) {
         if (r->gexec) cudaGraphExecDestroy(r->gexec);
@@ -1627,6 +1637,7 @@ int launch_run(Run* r, const snc_lif* lif, int mode, int path, cudaStream_t st) 
           r->gexec_mode = mode;
           r->gexec_lif = *lif;
           r->gexec_stream = st;
+          r->gexec_wait_ns = a.wait_ns;
         }
       }
     }

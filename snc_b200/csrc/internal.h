@@ -15,6 +15,19 @@ namespace sncb {
 void set_error(const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);  // records and maps to a status
 
+// Failure injection on the host (api.cu): true when this device allocation is
+// to fail (SNC_B200_FAIL_ALLOC / snc_b200_inject_alloc_failure).
+bool alloc_fault();
+
+// Wait bound and injected stall of a launch with grid barriers (api.cu):
+// ns = 0 is the default bound; stall > 0 makes every grid wait of that launch
+// run out.  consume: take one pending stall.
+struct WaitCtl {
+  unsigned long long ns;
+  unsigned stall;
+};
+WaitCtl take_wait_ctl(bool consume);
+
 #define SNCB_CUDA(call)                                  \
   do {                                                   \
     cudaError_t e_ = (call);                             \
@@ -25,6 +38,7 @@ template <typename T>
 int dev_upload(T** d, const T* h, size_t n) {
   *d = nullptr;
   if (n == 0) n = 1;
+  if (alloc_fault()) { set_error("device allocation failed (injected)"); return SNC_B200_ENOMEM; }
   SNCB_CUDA(cudaMalloc(reinterpret_cast<void**>(d), n * sizeof(T)));
   if (h) SNCB_CUDA(cudaMemcpy(*d, h, n * sizeof(T), cudaMemcpyHostToDevice));
   return SNC_B200_OK;
@@ -34,6 +48,7 @@ template <typename T>
 int dev_alloc(T** d, size_t n) {
   *d = nullptr;
   if (n == 0) n = 1;
+  if (alloc_fault()) { set_error("device allocation failed (injected)"); return SNC_B200_ENOMEM; }
   SNCB_CUDA(cudaMalloc(reinterpret_cast<void**>(d), n * sizeof(T)));
   return SNC_B200_OK;
 }
@@ -174,6 +189,7 @@ struct Run {
   int gexec_mode = -1;
   snc_lif gexec_lif{};
   cudaStream_t gexec_stream = nullptr;
+  unsigned long long gexec_wait_ns = 0;  // wait bound baked into the graph
   cudaStream_t own_stream = nullptr;  // stands in for the legacy default stream
   bool graph_refused = false;         // stream capture failed once; launch directly
   bool used_graph = false;            // the last launch went through the graph

@@ -365,6 +365,7 @@ int DevBuf::reserve(size_t n) {
   if (n <= cap) return SNC_B200_OK;
   const size_t want = std::max(n, cap + cap / 2);
   release();
+  if (alloc_fault()) { set_error("device allocation failed (injected)"); return SNC_B200_ENOMEM; }
   SNCB_CUDA(cudaMalloc(&p, want));
   cap = want;
   return SNC_B200_OK;
@@ -804,6 +805,7 @@ int oneshot_forward(const Graph* g, const snc_input_event* ev, size_t n_ev, int 
   if (cudaMemcpy(&err, in.d_err, 4, cudaMemcpyDeviceToHost) == cudaSuccess && err && !rc) {
     set_error("schedule entries exceeded their bound");
     rc = SNC_B200_EOVERFLOW;
+    if (stats) stats->overflow = 1;
   }
   return rc;
 }

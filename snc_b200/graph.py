@@ -1,6 +1,6 @@
 """Host-side spiking graph: the reference's ``SNNGraph`` CSR as numpy arrays.
 
-Mirrors ``struct SNNGraph`` (include/snc/snn_graph.hpp:114-148): a CSR over
+Mirrors ``struct SNNGraph`` (include/snc/snn_graph.hpp:43-77): a CSR over
 OUTGOING synapses (``row_ptr[N+1]``, ``post_ids[S]``, ``weights[S]``,
 ``delays[S]``, ``branch_ids[S]``) plus per-neuron ``role`` (0 internal, 1
 input, 2 output), ``sign`` (+1/-1, Dale's sign on the pre neuron) and
@@ -193,7 +193,7 @@ def save_sncg(g: SNNGraph, path, with_weights=True) -> None:
 
 
 # InputEvent {int sample_id, channel_id, time; float amplitude}
-# (include/snc/encoders.hpp:224-229), 16 bytes, same layout as the C ABI.
+# (include/snc/encoders.hpp:21-26), 16 bytes, same layout as the C ABI.
 EVENT_DTYPE = np.dtype([("sample_id", "<i4"), ("channel_id", "<i4"),
                         ("time", "<i4"), ("amplitude", "<f4")])
 

@@ -272,3 +272,72 @@ def test_layout_transpose_matches_torch():
     np.testing.assert_array_equal(BP._to_tnb(y).cpu().numpy(), y.permute(0, 2, 1).contiguous().cpu().numpy())
     z = torch.randn(5, 33, 129, generator=gen).to(DEV)
     np.testing.assert_array_equal(BP._from_tnb(z).cpu().numpy(), z.permute(0, 2, 1).contiguous().cpu().numpy())
+
+
+def _grad_errors(g, r):
+    """(largest |g - r| over the largest |r|, largest elementwise |g - r| / |r|
+    over the entries with |r| >= 1e-2 of the largest)."""
+    scale = float(r.abs().max())
+    maxnorm = float((g - r).abs().max()) / max(scale, 1e-30)
+    big = r.abs() >= 1e-2 * scale
+    elem = float(((g - r).abs()[big] / r.abs()[big]).max()) if bool(big.any()) else 0.0
+    return maxnorm, elem
+
+
+def _bench_shape_case(pre, post, delays, N, w, ext, ckpt, seed):
+    """Core spikes and weight / drive gradients of the custom kernels against
+    the CPU autograd restatement on the same weights and drive."""
+    gen = torch.Generator().manual_seed(seed)
+    proj = torch.randn(ext.shape, generator=gen)
+    wt = w.clone().requires_grad_(True)
+    et = ext.clone().requires_grad_(True)
+    s_ref = BR.core_forward(wt, et, torch.as_tensor(pre).long(), torch.as_tensor(post).long(),
+                            torch.as_tensor(delays).long(), 1.0, 0.95, 25.0)
+    (s_ref * proj).sum().backward()
+    core = BP.SpikingCore(N, np.asarray(pre), np.asarray(post), np.asarray(delays), device=DEV)
+    wg = w.to(DEV).clone().requires_grad_(True)
+    eg = ext.to(DEV).clone().requires_grad_(True)
+    s = BP.spiking_core(wg, eg, core, 1.0, 0.95, 25.0, ckpt, False)
+    (s * proj.to(DEV)).sum().backward()
+    assert float(s_ref.sum()) > 0
+    assert torch.equal(s.detach().cpu(), s_ref.detach())
+    return _grad_errors(wg.grad.cpu(), wt.grad), _grad_errors(eg.grad.cpu(), et.grad)
+
+
+def test_mnist_like_bench_shape_gradients():
+    """The benchmark's mnist-like BPTT configuration (784 Poisson -> 512 ->
+    512 LIF, local sparse, delays 1-4, batch 128, checkpoints every 10 steps)
+    with its own graph, weights and input spikes, T cut from 100 to 50 so the
+    CPU autograd model stays small: forward spikes identical; weight and
+    drive gradients within 1e-4, both relative to the largest gradient and
+    elementwise over entries of at least 1e-2 of the largest."""
+    c4 = W.bptt_mnist_like(T=50)
+    model = BP.DelayedSNN(c4["N"], c4["pre"], c4["post"], c4["delays"], c4["n_in"],
+                          c4["readout_ids"], 10, thr=1.0, decay=0.95, surrogate_scale=25.0,
+                          ckpt_every=10)
+    T, B = c4["spikes"].shape[:2]
+    assert B == 128
+    ext = torch.zeros(T, B, c4["N"])
+    ext[:, :, :c4["n_in"]] = torch.as_tensor(c4["spikes"])
+    (gw_max, gw_el), (ge_max, ge_el) = _bench_shape_case(c4["pre"], c4["post"], c4["delays"], c4["N"],
+                                                         model.w.detach(), ext, 10, 4)
+    assert gw_max <= 1e-4 and gw_el <= 1e-4, (gw_max, gw_el)
+    assert ge_max <= 1e-4 and ge_el <= 1e-4, (ge_max, ge_el)
+
+
+def test_char_lm_bench_shape_gradients():
+    """The benchmark's char-LM configuration (4096 recurrent LIF, fan-in 64,
+    delays 1-8, batch 64, checkpoints every 16 steps) with its own graph,
+    weights and embedded Zipf tokens, T cut from 256 to 48: the same bars as
+    the mnist-like case."""
+    c5 = W.char_lm(T=48)
+    torch.manual_seed(0)
+    net = BP.SpikingLM(c5["vocab"], c5["H"], c5["pre"], c5["post"], c5["delays"], w_scale=2.0,
+                       ckpt_every=16)
+    with torch.no_grad():
+        ext = net.embed(torch.as_tensor(c5["x"])).transpose(0, 1).contiguous()
+    assert ext.shape[1] == 64
+    (gw_max, gw_el), (ge_max, ge_el) = _bench_shape_case(c5["pre"], c5["post"], c5["delays"], c5["H"],
+                                                         net.w_rec.detach(), ext, 16, 5)
+    assert gw_max <= 1e-4 and gw_el <= 1e-4, (gw_max, gw_el)
+    assert ge_max <= 1e-4 and ge_el <= 1e-4, (ge_max, ge_el)

@@ -11,10 +11,11 @@ import numpy as np
 import pytest
 import torch
 
+from oracle import REF_ROOT
 from oracle import bptt_ref as BR
 from snc_b200 import workloads as W
 
-REF_PY = "/root/reference/python"
+REF_PY = os.path.join(REF_ROOT, "python")
 needs_ref_py = pytest.mark.skipif(not os.path.isdir(os.path.join(REF_PY, "snc")),
                                   reason="reference python bridge absent")
 

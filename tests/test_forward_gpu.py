@@ -208,3 +208,59 @@ def test_graph_without_synapses(pname, path, force):
     assert int(ref["spikes"].sum()) > 0 and int(ref["events"].sum()) == 0
     out = run_gpu(g, ev, steps, lif, R.MODE_SORT, path, force_grid=force)
     assert_exact(out, ref)
+
+
+# ---- the benchmarked configurations at their own sizes ---------------------
+
+@pytest.fixture(scope="module")
+def rec100k_bench():
+    """The bench's headline input: rec100k seed 1, one sample of 1000 steps
+    with Poisson drive seed 1, tau_mem 20 with subtractive reset."""
+    g = W.rec100k_graph(seed=1)
+    ev, steps = W.rec100k_inputs(g, 1, 1000, seed=1)
+    lif = W.lif_tau20()
+    return g, ev, steps, lif, O.forward_batched(g, ev, steps, lif)
+
+
+@pytest.mark.parametrize("path,graph", [(R.PATH_PLAIN, False), (R.PATH_PERSISTENT, True),
+                                        (R.PATH_PERSISTENT, False)])
+def test_rec100k_bench_input_sort_bit_exact(rec100k_bench, path, graph):
+    g, ev, steps, lif, ref = rec100k_bench
+    out = run_gpu(g, ev, steps, lif, R.MODE_SORT, path, cuda_graph=graph, repeat=2)
+    assert int(ref["spikes"].sum()) > 100_000
+    assert_exact(out, ref)
+
+
+@pytest.mark.parametrize("mode", [R.MODE_ATOMIC, R.MODE_BUCKET])
+@pytest.mark.parametrize("path", [R.PATH_PLAIN, R.PATH_PERSISTENT])
+def test_rec100k_bench_input_unordered(rec100k_bench, mode, path):
+    g, ev, steps, lif, ref = rec100k_bench
+    out = run_gpu(g, ev, steps, lif, mode, path, cuda_graph=(path == R.PATH_PERSISTENT))
+    assert spike_count_agreement(out["spikes"], ref["spikes"]) >= 0.999
+    assert spike_count_agreement(out["events"], ref["events"]) >= 0.999
+
+
+@pytest.fixture(scope="module")
+def audio700_all():
+    g = W.audio700_graph()
+    ev, steps = W.audio700_inputs(256)
+    lif = W.lif_tau20()
+    return g, ev, steps, lif, O.forward_batched(g, ev, steps, lif)
+
+
+@pytest.mark.parametrize("path,force,graph", [(R.PATH_PERSISTENT, False, True),
+                                              (R.PATH_PERSISTENT, True, False),
+                                              (R.PATH_PLAIN, False, False)])
+def test_audio700_all_256_samples_sort_bit_exact(audio700_all, path, force, graph):
+    """C3 as benchmarked: all 256 uneven samples (50-1000 steps) in one
+    launch, rasters and potentials bit-identical on every path."""
+    g, ev, steps, lif, ref = audio700_all
+    out = run_gpu(g, ev, steps, lif, R.MODE_SORT, path, force_grid=force, cuda_graph=graph)
+    assert len(steps) == 256
+    assert_exact(out, ref)
+
+
+def test_audio700_all_256_samples_atomic(audio700_all):
+    g, ev, steps, lif, ref = audio700_all
+    out = run_gpu(g, ev, steps, lif, R.MODE_ATOMIC, R.PATH_PERSISTENT, cuda_graph=True)
+    assert spike_count_agreement(out["spikes"], ref["spikes"]) >= 0.999

@@ -5,6 +5,7 @@ import subprocess
 import numpy as np
 import pytest
 
+from oracle import REF_ROOT
 from oracle import oracle as O
 from snc_b200 import graph as G
 from snc_b200 import workloads as W
@@ -46,7 +47,7 @@ def test_reads_reference_snc_export_output(tmp_path):
     g = G.graph_from_sncg(d)
     assert g.validate() == ""
     assert g.num_input_channels == d["n_in"] == 784 and g.num_output_channels == d["n_out"] == 10
-    ref_loader = "/root/reference/python/snc/graph.py"
+    ref_loader = os.path.join(REF_ROOT, "python", "snc", "graph.py")
     if os.path.exists(ref_loader):
         import importlib.util
         spec = importlib.util.spec_from_file_location("ref_graph", ref_loader)

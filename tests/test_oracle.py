@@ -115,7 +115,7 @@ def test_batched_equals_per_sample():
 @pytest.mark.parametrize("train_hidden", [False, True])
 def test_eprop_restatement_matches_reference_trainer(train_hidden):
     """Minibatch e-prop at batch 1 vs the reference per-sample Trainer
-    (src/training/trainer.cpp:161-317).  The Trainer accumulates E in
+    (src/training/trainer.cpp:154-208).  The Trainer accumulates E in
     double, the minibatch rule in fp32, hence the tolerance."""
     g = O.ref_generate("static-snc", [40, 60, 5], synapse_budget=1500, weight=0.5, delay=2,
                        inhib=0.2, seed=3)
