@@ -57,7 +57,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--mode", default="auto", choices=["auto", "atomic", "bucket", "sort"])
     p.add_argument("--no-extra", action="store_true", help="skip the plain / sort / cpu legs")
-    p.add_argument("--leg", choices=["bptt", "bptt-custom", "configs"],
+    p.add_argument("--leg", choices=["bptt", "bptt-custom", "configs", "reference-gpu"],
                    help="run only this extra leg on one GPU and print its JSON (for profiling)")
     return p.parse_args()
 
@@ -355,6 +355,166 @@ def config_legs(reps=3):
     return out
 
 
+REF_GPU_LIB = os.path.join(ROOT, "snc_b200", "adapter", "_build", "libsncref_gpu.so")
+REF_BACKENDS = {"atomic": 2, "bucket": 3, "sort": 4}  # the reference's Backend::Cuda* values
+
+
+class RefGpu:
+    """The reference's own GPU implementation -- src/runtime/cuda_backend.cu
+    and src/training/cuda_trainer.cu unchanged, compiled for sm_100a with its
+    CPU sources into snc_b200/adapter/_build/libsncref_gpu.so (make -C
+    snc_b200/adapter side) -- reached through its public API (snc::forward
+    with the cuda-* backends, snc::cudatrain) by ref_gpu_shim.cpp."""
+
+    def __init__(self):
+        import ctypes as C
+        self.C = C
+        self.L = C.CDLL(REF_GPU_LIB)
+        P, I, F = C.c_void_p, C.c_int, C.c_float
+        self.L.refgpu_graph_create.restype = P
+        self.L.refgpu_graph_create.argtypes = [I, I] + [P] * 7
+        self.L.refgpu_graph_destroy.argtypes = [P]
+        self.L.refgpu_available.restype = I
+        self.L.refgpu_forward.restype = C.c_double
+        self.L.refgpu_forward.argtypes = [P, P, C.c_int64, I, F, F, F, I, I, P, P, P, P, P]
+        self.L.refgpu_train.restype = C.c_double
+        self.L.refgpu_train.argtypes = [P, I, F, F, F, I, F, F, F, I, I, I, P, P, I, I, P, P]
+
+    def graph(self, g):
+        p = lambda a: a.ctypes.data  # noqa: E731
+        arrs = [np.ascontiguousarray(a, t) for a, t in
+                ((g.row_ptr, np.int32), (g.post_ids, np.int32), (g.weights, np.float32),
+                 (g.delays, np.int32), (g.role, np.uint8), (g.sign, np.int8), (g.channel, np.int32))]
+        h = self.L.refgpu_graph_create(g.num_neurons, g.num_synapses, *[p(a) for a in arrs])
+        return h, arrs
+
+    def forward(self, h, n_out, ev, steps, lif, mode):
+        C = self.C
+        ev = np.ascontiguousarray(ev)
+        logits = np.zeros(max(1, n_out), np.float32)
+        sp, en, used, wall = C.c_int64(), C.c_int64(), C.c_int(), C.c_double()
+        ms = self.L.refgpu_forward(h, ev.ctypes.data, ev.shape[0], int(steps), lif.threshold, lif.decay,
+                                   lif.reset, lif.refractory, REF_BACKENDS[mode], logits.ctypes.data,
+                                   C.byref(sp), C.byref(en), C.byref(used), C.byref(wall))
+        if used.value != REF_BACKENDS[mode]:
+            raise RuntimeError(f"reference cuda-{mode} fell back to the CPU")
+        return {"ms": ms, "wall_ms": wall.value, "spikes": sp.value, "events": en.value}
+
+
+def reference_gpu_leg(budget_s=40.0):
+    """The reference's GPU kernels beside this backend's on the same B200 and
+    the same inputs, in the reference's LIF semantics (reset to 0: it has no
+    subtractive reset), forward of every delivery mode:
+      C1 ff784 (64 samples x 50 steps), C2 rec100k (1 x 1000 steps),
+      C3 audio700 (the first 32 of the 256 uneven samples; the reference runs
+      one sample per call) --
+    the reference per sample through snc::forward (its RunStats.ms: the step
+    loop, launches included; and the wall time of the call, which also
+    uploads the graph and frees it), this backend's plain path (one sample
+    per launch sequence, like the reference) and persistent path (device
+    time).  Then one e-prop minibatch on C3's graph: the reference's
+    cudatrain::train_epoch on 32 samples of mean length (its trainer needs
+    one length per session) beside this backend's minibatch on the same
+    samples' uneven lengths, as sample-steps per second."""
+    if not os.path.exists(REF_GPU_LIB):
+        return {"unavailable": "snc_b200/adapter/_build/libsncref_gpu.so not built "
+                               "(make -C snc_b200/adapter side needs the reference sources)"}
+    import torch
+    from snc_b200 import eprop as EP
+    from snc_b200 import runtime as R
+    from snc_b200 import workloads as W
+    ref = RefGpu()
+    if ref.L.refgpu_available() != 1:
+        return {"unavailable": "the reference's cuda::available() is false"}
+    lif0 = W.lif_tau20()
+    lif = R.LIFParams(threshold=lif0.threshold, decay=lif0.decay, reset=0.0,
+                      refractory=lif0.refractory, reset_mode=0)
+    out = {"lif": "threshold 1, decay exp(-1/20), reset to 0, refractory 0 (the reference's semantics)"}
+    t_start = time.perf_counter()
+    for name, g, (ev, steps) in (("C1_ff784", W.ff784_graph(), W.ff784_inputs(64)),
+                                 ("C2_rec100k", W.rec100k_graph(seed=1), None),
+                                 ("C3_audio700_32", W.audio700_graph(), W.audio700_inputs(256))):
+        if name == "C2_rec100k":
+            ev, steps = W.rec100k_inputs(g, 1, 1000, seed=1)
+        if name.startswith("C3"):
+            keep = np.arange(32)
+            ev = ev[np.isin(ev["sample_id"], keep)]
+            steps = steps[:32]
+        B = len(steps)
+        per = [ev[ev["sample_id"] == b] for b in range(B)]
+        h, _keep = ref.graph(g)
+        dg = R.DeviceGraph(g)
+        di = R.DeviceInputs(dg, ev, steps)
+        run = R.Run(dg, di, cuda_graph=True)
+        leg = {"samples": B, "sample_steps": int(np.sum(steps))}
+        for mode in ("atomic", "bucket", "sort"):
+            if time.perf_counter() - t_start > budget_s:
+                leg[f"reference_{mode}"] = {"skipped": f"leg budget {budget_s:.0f} s spent"}
+                continue
+            loop_ms = wall_ms = 0.0
+            sp = en = 0
+            for b in range(B):
+                r = ref.forward(h, g.num_output_channels, per[b], steps[b], lif, mode)
+                loop_ms += r["ms"]
+                wall_ms += r["wall_ms"]
+                sp += r["spikes"]
+                en += r["events"]
+            leg[f"reference_{mode}"] = {"loop_ms": loop_ms, "call_ms": wall_ms, "spikes": sp,
+                                        "events": en, "events_per_s_loop": en / (loop_ms / 1e3)}
+            m = {"atomic": R.MODE_ATOMIC, "bucket": R.MODE_BUCKET, "sort": R.MODE_SORT}[mode]
+            for p in (R.PATH_PLAIN, R.PATH_PERSISTENT):
+                ms = []
+                for _ in range(3):
+                    run.launch(lif, mode=m, path=p)
+                    o = run.fetch()
+                    ms.append(o["ms"])
+                best = min(ms[1:])
+                leg[f"b200_{mode}_{R.PATH_NAMES[p]}"] = {
+                    "ms": best, "spikes": int(o["total_spikes"]), "events": int(o["total_events"]),
+                    "events_per_s": o["total_events"] / (best / 1e3),
+                    "speedup_vs_reference_loop": loop_ms / best}
+        out[name] = leg
+        run.release()
+        di.release()
+        dg.release()
+        ref.L.refgpu_graph_destroy(h)
+    # e-prop minibatch on C3's graph
+    g = W.audio700_graph()
+    ev, steps = W.audio700_inputs(32)
+    T_mean = int(round(float(np.mean(steps))))
+    feats = np.minimum(np.random.default_rng(3).lognormal(np.log(0.01) - 0.5, 1.0, (32, 700)),
+                       1.0).astype(np.float32)
+    labels = np.random.default_rng(5).integers(0, g.num_output_channels, 32).astype(np.int32)
+    h, _keep = ref.graph(g)
+    C = ref.C
+    sp, en = C.c_int64(), C.c_int64()
+    ref.L.refgpu_train(h, T_mean, lif.threshold, lif.decay, lif.reset, lif.refractory, 1.0, 1.0, 0.3,
+                       32, 700, g.num_output_channels, feats.ctypes.data, labels.ctypes.data, 32, 1,
+                       C.byref(sp), C.byref(en))  # warm-up epoch
+    ms_ref = ref.L.refgpu_train(h, T_mean, lif.threshold, lif.decay, lif.reset, lif.refractory, 1.0,
+                                1.0, 0.3, 32, 700, g.num_output_channels, feats.ctypes.data,
+                                labels.ctypes.data, 32, 3, C.byref(sp), C.byref(en)) / 3
+    ref.L.refgpu_graph_destroy(h)
+    cfg = EP.TrainConfig(lif=lif, lr=1.0, trace_decay=lif.decay, mode=R.MODE_ATOMIC)
+    sess = EP.create(g, cfg, 32)
+    wall = []
+    for _ in range(4):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sess.run_batch(ev, steps, labels, train=True)
+        wall.append(1e3 * (time.perf_counter() - t0))
+    sess.release()
+    ss_ref, ss_ours = 32 * T_mean, int(np.sum(steps))
+    out["eprop_C3_minibatch32"] = {
+        "reference_epoch_ms": ms_ref, "reference_T": T_mean,
+        "reference_sample_steps_per_s": ss_ref / (ms_ref / 1e3),
+        "b200_wall_ms": min(wall[1:]), "b200_sample_steps": ss_ours,
+        "b200_sample_steps_per_s": ss_ours / (min(wall[1:]) / 1e3),
+        "note": "reference: Poisson drawn on the GPU by cuRAND, one T per session; "
+                "b200: host-encoded events, uneven T, atomic delivery"}
+    return out
+
+
 def bptt_leg(steps=3, warmup=2, lm=True, with_reference=True):
     """BPTT step (forward + backward) of the custom kernels against the
     PyTorch-autograd bridge (oracle/bptt_ref.py, the reference bridge's model
@@ -571,6 +731,7 @@ def our_arm(args):
         extra["parity"] = parity_leg(dg, di, g, ev, lif, mode, timed_out,
                                      ref_counts if cpu["kind"] == "reference" else None)
         extra["configs"] = config_legs()
+        extra["reference_gpu"] = reference_gpu_leg()
         extra["bptt"] = bptt_leg()
 
     if rank == 0:
@@ -599,7 +760,7 @@ def main():
     args = parse()
     if args.leg:
         legs = {"bptt": bptt_leg, "bptt-custom": lambda: bptt_leg(with_reference=False),
-                "configs": config_legs}
+                "configs": config_legs, "reference-gpu": reference_gpu_leg}
         print(json.dumps({args.leg: legs[args.leg]()}), flush=True)
         return 0
     if args.impl == "reference":

@@ -241,12 +241,53 @@ int snc_b200_forward_batched(const snc_b200_graph* graph, const snc_input_event*
                              const snc_lif* lif, int mode, float* logits, int64_t* spikes,
                              int64_t* events_out, snc_run_stats* stats);
 
-/* ---- delivery autotuner ------------------------------------------------------
- * Time every (mode, path, block size) candidate on this graph with the given
- * inputs, cache the winner per graph signature and return it.  Later AUTO
- * launches on graphs with the same signature reuse the choice. */
+/* ---- launch shapes and the delivery autotuner ---------------------------------
+ * No reference counterpart: the reference picks its backend by a flag
+ * (src/bench/snc_bench.cpp:301-317).
+ *
+ * A launch's shape on the persistent path: tier 0 runs one sample per CTA
+ * with the sample's whole state in shared memory (when it fits), tier 1 runs
+ * every SM on a wave of samples in lockstep; on tier 1, block_threads threads
+ * per block (a multiple of 32 in [512, 768]), wave samples per wave and the
+ * delay-ring slices in shared (ring_smem 1) or global (0) memory.  -1 / 0 in
+ * a field: chosen automatically.  ms is filled by the autotuner. */
+typedef struct {
+  int32_t mode;          /* SNC_B200_MODE_ATOMIC / _BUCKET / _SORT */
+  int32_t path;          /* SNC_B200_PATH_PLAIN / _PERSISTENT */
+  int32_t tier;          /* persistent path: 0 sample per CTA, 1 all SMs; -1 automatic */
+  int32_t block_threads; /* tier 1: threads per block; 0 automatic */
+  int32_t wave;          /* tier 1: samples in lockstep; 0 as many as fit */
+  int32_t ring_smem;     /* tier 1 (bucket, sort): 1 shared, 0 global; -1 automatic */
+  float ms;              /* autotuner: device time of the candidate's timed launch */
+} snc_launch_config;
+
+/* Fix the shape of this run's launches (mode and path of cfg are only used to
+ * check it; they stay arguments of snc_b200_run_launch).  NULL: back to
+ * automatic.  SNC_B200_EUNSUPPORTED for a shape the graph or device cannot
+ * take (tier 0 when a sample does not fit one CTA, ring slices that do not
+ * fit). */
+int snc_b200_run_configure(snc_b200_run* r, const snc_launch_config* cfg);
+
+/* Time every candidate on this graph and these inputs: each delivery mode on
+ * the plain path (batches of at most 8 samples), on tier 0 (atomic and sort,
+ * when a sample fits one CTA) and on tier 1 over block_threads {the block's
+ * neuron count rounded to 32, 512, 768}, wave {as many as fit, 1 (batches of
+ * 2-64)} and ring placement {shared, global} (bucket, sort); batches above 64
+ * samples time tier 1 in its default shape only.  Each candidate is launched
+ * twice and its second device time kept.  The fastest is cached under the
+ * graph's content hash and the batch's sample and step counts, and AUTO
+ * launches with that key use its mode, path and shape.  cand[0 .. max_cand)
+ * receives the candidates, *n_cand their number, *best the winner's index
+ * (any may be NULL). */
+int snc_b200_autotune_ex(const snc_b200_graph* g, const snc_b200_inputs* in, const snc_lif* lif,
+                         snc_launch_config* cand, int32_t max_cand, int32_t* n_cand, int32_t* best);
+/* snc_b200_autotune_ex returning the winner's mode, path and threads per
+ * block (1024 for tier 0, 512 for the plain path). */
 int snc_b200_autotune(const snc_b200_graph* g, const snc_b200_inputs* in, const snc_lif* lif,
                       int* mode, int* path, int* block_threads);
+/* 1 and the cached winner in *out when this graph and batch shape were tuned,
+ * 0 otherwise. */
+int snc_b200_autotune_lookup(const snc_b200_graph* g, const snc_b200_inputs* in, snc_launch_config* out);
 
 /* ---- minibatch e-prop (replaces snc::cudatrain, cuda_trainer.hpp:26-57) ----
  * The learning rule of src/training/cuda_trainer.cu: LIF + triangular

@@ -40,6 +40,12 @@ class Lif(C.Structure):
                 ("refractory", C.c_int32), ("reset_mode", C.c_int32)]
 
 
+class LaunchConfig(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("path", C.c_int32), ("tier", C.c_int32),
+                ("block_threads", C.c_int32), ("wave", C.c_int32), ("ring_smem", C.c_int32),
+                ("ms", C.c_float)]
+
+
 class RunStats(C.Structure):
     _fields_ = [("spikes", C.c_int64), ("synaptic_events", C.c_int64), ("overflow", C.c_int32),
                 ("ms", C.c_double)]
@@ -75,6 +81,9 @@ SIGNATURES = {
     "snc_b200_forward": (C.c_int, [P, P, P, C.c_size_t, I32, P, C.c_int, P, P]),
     "snc_b200_forward_batched": (C.c_int, [P, P, C.c_size_t, I32, P, P, C.c_int, P, P, P, P]),
     "snc_b200_autotune": (C.c_int, [P, P, P, P, P, P]),
+    "snc_b200_autotune_ex": (C.c_int, [P, P, P, P, I32, P, P]),
+    "snc_b200_autotune_lookup": (C.c_int, [P, P, P]),
+    "snc_b200_run_configure": (C.c_int, [P, P]),
     "snc_b200_eprop_create": (C.c_int, [P, P, P, I32, P, P, P]),
     "snc_b200_eprop_release": (C.c_int, [P]),
     "snc_b200_eprop_path": (C.c_int, [P]),

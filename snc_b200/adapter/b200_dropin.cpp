@@ -1,6 +1,15 @@
 // Reference-side drop-in: the reference's own CUDA hooks implemented over the
 // C ABI of libsnc_b200.so.
 //
+// Two builds of this file (snc_b200/adapter/Makefile):
+//   default          the link-time swap described below: snc::cuda and
+//                    snc::cudatrain ARE the B200 backend;
+//   SNC_B200_BESIDE  against the reference's backend table extended by
+//                    beside.py: this file defines only snc::b200 (the
+//                    b200-atomic / b200-bucket / b200-sort backends), and the
+//                    reference's own cuda_backend.cu and cuda_trainer.cu are
+//                    linked unchanged beside it.
+//
 //   snc::cuda::available / snc::cuda::forward   include/snc/runtime.hpp:61-69
 //   snc::cudatrain::*                           include/snc/cuda_trainer.hpp:26-57
 //
@@ -40,6 +49,7 @@ static_assert(sizeof(snc::InputEvent) == sizeof(snc_input_event), "InputEvent la
 
 namespace snc {
 
+#ifndef SNC_B200_BESIDE
 struct CudaTrainSession {
   const SNNGraph* g = nullptr;
   TrainConfig cfg;
@@ -47,6 +57,7 @@ struct CudaTrainSession {
   snc_b200_graph* gh = nullptr;
   snc_b200_eprop* s = nullptr;
 };
+#endif
 
 namespace {
 
@@ -111,14 +122,23 @@ snc_b200_graph* cached_graph(const SNNGraph& g) {
 }
 
 int mode_of(Backend b) {
+#ifdef SNC_B200_BESIDE
+  if (b == Backend::B200Atomic) return SNC_B200_MODE_ATOMIC;
+  if (b == Backend::B200Bucket) return SNC_B200_MODE_BUCKET;
+#else
   if (b == Backend::CudaAtomic) return SNC_B200_MODE_ATOMIC;
   if (b == Backend::CudaBucket) return SNC_B200_MODE_BUCKET;
+#endif
   return SNC_B200_MODE_SORT;
 }
 
 }  // namespace
 
+#ifdef SNC_B200_BESIDE
+namespace b200 {
+#else
 namespace cuda {
+#endif
 
 bool available() { return snc_b200_available() == 1; }
 
@@ -142,6 +162,9 @@ bool forward(const SNNGraph& g, const std::vector<InputEvent>& events, int num_s
   return true;
 }
 
+#ifdef SNC_B200_BESIDE
+}  // namespace b200
+#else
 }  // namespace cuda
 
 namespace cudatrain {
@@ -305,4 +328,5 @@ void collect_stats(const CudaTrainSession* s, std::vector<long long>& syn, std::
 }
 
 }  // namespace cudatrain
+#endif  // SNC_B200_BESIDE
 }  // namespace snc

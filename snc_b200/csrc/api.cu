@@ -109,9 +109,44 @@ static void free_graph(Graph* g) {
     dev_free(p);
 }
 
+// 64-bit content hash of a graph view (sizes and every array, weights by
+// their bits): the autotuner's cache key.  Words are folded pairwise with a
+// multiply-xorshift mix, one pass over the arrays.
+static unsigned long long graph_hash(const snc_graph_view* v) {
+  unsigned long long h = 0x9E3779B97F4A7C15ull ^ ((unsigned long long)v->num_neurons << 32) ^
+                         (unsigned)v->num_synapses;
+  auto mix = [&h](unsigned long long x) {
+    h ^= x + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 31;
+  };
+  auto words = [&mix](const void* p, size_t bytes) {
+    const unsigned char* c = static_cast<const unsigned char*>(p);
+    size_t i = 0;
+    for (; i + 8 <= bytes; i += 8) {
+      unsigned long long x;
+      std::memcpy(&x, c + i, 8);
+      mix(x);
+    }
+    unsigned long long tail = 0;
+    std::memcpy(&tail, c + i, bytes - i);
+    mix(tail ^ ((unsigned long long)bytes << 56));
+  };
+  const size_t n = (size_t)v->num_neurons, m = (size_t)v->num_synapses;
+  words(v->row_ptr, 4 * (n + 1));
+  words(v->post_ids, 4 * m);
+  words(v->weights, 4 * m);
+  words(v->delays, 4 * m);
+  words(v->role, n);
+  words(v->sign, n);
+  words(v->channel, 4 * n);
+  return h;
+}
+
 static int upload_graph(const snc_graph_view* v, Graph* g) {
   int rc = validate_view(v);
   if (rc) return rc;
+  g->hash = graph_hash(v);
   const int n = v->num_neurons, m = v->num_synapses;
   int dev = 0;
   cudaGetDevice(&dev);
@@ -287,16 +322,38 @@ int fetch_run(Run* r, float* logits, int64_t* spikes, int64_t* events, uint32_t*
 }
 
 // ---- autotuner --------------------------------------------------------------
+// Tuned launches, keyed by the graph's content hash and the batch's shape
+// (samples, total steps): a graph of similar size but other contents is tuned
+// on its own.
+struct TuneKey {
+  unsigned long long hash;
+  int B;
+  long long steps;
+  bool operator<(const TuneKey& o) const {
+    if (hash != o.hash) return hash < o.hash;
+    if (B != o.B) return B < o.B;
+    return steps < o.steps;
+  }
+};
 static std::mutex g_tune_mu;
-static std::map<long long, std::pair<int, int>> g_tune_cache;
+static std::map<TuneKey, snc_launch_config> g_tune_cache;
 
-int resolve_auto(const Graph* g, const Inputs* in, int* mode, int* path) {
+static TuneKey tune_key(const Graph* g, const Inputs* in) {
+  return TuneKey{g->hash, in->B, in->total_steps};
+}
+
+int resolve_auto(const Graph* g, const Inputs* in, int* mode, int* path, int* shape) {
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tune_cache.find(g->signature);
+    auto it = g_tune_cache.find(tune_key(g, in));
     if (it != g_tune_cache.end()) {
-      if (*mode == SNC_B200_MODE_AUTO) *mode = it->second.first;
-      if (*path == SNC_B200_PATH_AUTO) *path = it->second.second;
+      const snc_launch_config& c = it->second;
+      if (*mode == SNC_B200_MODE_AUTO) *mode = c.mode;
+      if (*path == SNC_B200_PATH_AUTO) *path = c.path;
+      shape[0] = c.tier;
+      shape[1] = c.block_threads;
+      shape[2] = c.wave;
+      shape[3] = c.ring_smem;
       return SNC_B200_OK;
     }
   }
@@ -304,7 +361,10 @@ int resolve_auto(const Graph* g, const Inputs* in, int* mode, int* path) {
   // heavily skewed (many sources hammer few targets), atomic otherwise.
   if (*path == SNC_B200_PATH_AUTO) *path = SNC_B200_PATH_PERSISTENT;
   if (*mode == SNC_B200_MODE_AUTO) *mode = g->fanin_cv > 1.0f ? SNC_B200_MODE_BUCKET : SNC_B200_MODE_ATOMIC;
-  (void)in;
+  shape[0] = -1;
+  shape[1] = 0;
+  shape[2] = 0;
+  shape[3] = -1;
   return SNC_B200_OK;
 }
 
@@ -505,34 +565,117 @@ int snc_b200_forward_batched(const snc_b200_graph* graph, const snc_input_event*
                          SNC_B200_PATH_PERSISTENT, logits, spikes, events_out, stats);
 }
 
-int snc_b200_autotune(const snc_b200_graph* g, const snc_b200_inputs* in, const snc_lif* lif,
-                      int* mode, int* path, int* block_threads) {
+int snc_b200_run_configure(snc_b200_run* r, const snc_launch_config* cfg) {
+  if (!r) { set_error("null run"); return SNC_B200_EINVAL; }
+  if (!cfg) {  // back to automatic shapes
+    r->cfg_tier = -1; r->cfg_threads = 0; r->cfg_wave = 0; r->cfg_rsm = -1;
+    r->cfg_explicit = false;
+    return SNC_B200_OK;
+  }
+  const int mode = cfg->mode >= 0 && cfg->mode <= SNC_B200_MODE_SORT ? cfg->mode : SNC_B200_MODE_SORT;
+  int rc = check_shape(r, mode, cfg->tier, cfg->block_threads, cfg->wave, cfg->ring_smem);
+  if (rc) return rc;
+  r->cfg_tier = cfg->tier;
+  r->cfg_threads = cfg->block_threads;
+  r->cfg_wave = cfg->wave;
+  r->cfg_rsm = cfg->ring_smem;
+  r->cfg_explicit = true;
+  return SNC_B200_OK;
+}
+
+int snc_b200_autotune_ex(const snc_b200_graph* g, const snc_b200_inputs* in, const snc_lif* lif,
+                         snc_launch_config* cand, int32_t max_cand, int32_t* n_cand, int32_t* best) {
   if (!g || !in || !lif) { set_error("null argument"); return SNC_B200_EINVAL; }
   Run r;
   int rc = create_run(g, in, 0, &r);
   if (rc) { free_run(&r); return rc; }
-  float best = 1e30f;
-  int bm = SNC_B200_MODE_ATOMIC, bp = SNC_B200_PATH_PERSISTENT;
-  for (int p = SNC_B200_PATH_PLAIN; p <= SNC_B200_PATH_PERSISTENT; ++p)
-    for (int m = SNC_B200_MODE_ATOMIC; m <= SNC_B200_MODE_SORT; ++m) {
-      float t = 0.f;
-      for (int rep = 0; rep < 2; ++rep) {  // first launch warms up
-        rc = launch_run(&r, lif, m, p, nullptr);
-        if (!rc) rc = fetch_run(&r, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
-        if (rc) break;
-        t = r.last_ms;
-      }
-      if (rc) { free_run(&r); return rc; }
-      if (t < best) { best = t; bm = m; bp = p; }
+  const int B = std::max(1, in->B);
+  // the candidates: every delivery mode on the plain path (small batches
+  // only: it runs the samples one after another), on the sample-per-CTA tier
+  // (when a sample fits one CTA; it has no bucket variant) and on the all-SM
+  // tier over its block sizes, wave sizes and ring placements
+  std::vector<snc_launch_config> cs;
+  auto add = [&](int m, int p, int tier, int thr, int wave, int rsm) {
+    snc_launch_config c{m, p, tier, thr, wave, rsm, 0.f};
+    if (p == SNC_B200_PATH_PERSISTENT && check_shape(&r, m, tier, thr, wave, rsm) != SNC_B200_OK) {
+      set_error("");
+      return;
     }
+    cs.push_back(c);
+  };
+  if (B <= 8)
+    for (int m = SNC_B200_MODE_ATOMIC; m <= SNC_B200_MODE_SORT; ++m)
+      add(m, SNC_B200_PATH_PLAIN, -1, 0, 0, -1);
+  for (int m : {SNC_B200_MODE_ATOMIC, SNC_B200_MODE_SORT})
+    if (check_shape(&r, m, 0, 0, 0, -1) == SNC_B200_OK) add(m, SNC_B200_PATH_PERSISTENT, 0, 0, 0, -1);
+  set_error("");
+  const int thr0 = std::max(512, std::min(768, (g->BS + 31) / 32 * 32));
+  std::vector<int> thrs = {thr0};
+  for (int t : {512, 768})
+    if (t != thr0) thrs.push_back(t);
+  std::vector<int> waves = {0};  // 0: as many samples as fit
+  if (B > 1 && B <= 64) waves.push_back(1);
+  const bool big = B > 64;  // bound the tuning time: default shape only
+  for (int m = SNC_B200_MODE_ATOMIC; m <= SNC_B200_MODE_SORT; ++m)
+    for (int rsm : (m == SNC_B200_MODE_ATOMIC ? std::vector<int>{0} : std::vector<int>{1, 0}))
+      for (int wave : waves)
+        for (int thr : thrs) {
+          if (big && (thr != thr0 || wave != 0)) continue;
+          add(m, SNC_B200_PATH_PERSISTENT, 1, thr, wave, rsm);
+        }
+  int bi = -1;
+  for (size_t i = 0; i < cs.size(); ++i) {
+    snc_launch_config& c = cs[i];
+    r.cfg_tier = c.tier; r.cfg_threads = c.block_threads; r.cfg_wave = c.wave; r.cfg_rsm = c.ring_smem;
+    r.cfg_explicit = true;
+    float t = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {  // the first launch warms up
+      rc = launch_run(&r, lif, c.mode, c.path, nullptr);
+      if (!rc) rc = fetch_run(&r, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+      if (rc) break;
+      t = r.last_ms;
+    }
+    if (rc) { free_run(&r); return rc; }
+    c.ms = t;
+    if (bi < 0 || t < cs[bi].ms) bi = (int)i;
+  }
   free_run(&r);
+  if (bi < 0) { set_error("autotune: no candidate"); return SNC_B200_EUNSUPPORTED; }
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune_cache[g->signature] = {bm, bp};
+    g_tune_cache[tune_key(g, in)] = cs[bi];
   }
-  if (mode) *mode = bm;
-  if (path) *path = bp;
-  if (block_threads) *block_threads = bp == SNC_B200_PATH_PERSISTENT && g->N <= 8192 ? 1024 : 512;
+  if (n_cand) *n_cand = (int32_t)cs.size();
+  if (best) *best = bi;
+  if (cand)
+    for (int i = 0; i < (int)cs.size() && i < max_cand; ++i) cand[i] = cs[i];
+  return SNC_B200_OK;
+}
+
+int snc_b200_autotune_lookup(const snc_b200_graph* g, const snc_b200_inputs* in, snc_launch_config* out) {
+  if (!g || !in) { set_error("null argument"); return SNC_B200_EINVAL; }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune_cache.find(tune_key(g, in));
+  if (it == g_tune_cache.end()) return 0;
+  if (out) *out = it->second;
+  return 1;
+}
+
+int snc_b200_autotune(const snc_b200_graph* g, const snc_b200_inputs* in, const snc_lif* lif,
+                      int* mode, int* path, int* block_threads) {
+  snc_launch_config best{};
+  int n = 0, bi = 0;
+  std::vector<snc_launch_config> cs(64);
+  int rc = snc_b200_autotune_ex(g, in, lif, cs.data(), (int)cs.size(), &n, &bi);
+  if (rc) return rc;
+  best = cs[bi];
+  if (mode) *mode = best.mode;
+  if (path) *path = best.path;
+  if (block_threads)
+    *block_threads = best.path == SNC_B200_PATH_PLAIN ? 512
+                     : best.tier == 0 ? 1024
+                     : best.block_threads > 0 ? best.block_threads
+                                              : std::max(512, std::min(768, (g->BS + 31) / 32 * 32));
   return SNC_B200_OK;
 }
 

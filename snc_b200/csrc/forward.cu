@@ -1444,11 +1444,15 @@ struct GPlan {
   size_t smem;
 };
 
-static GPlan plan_tier_g(const Graph* g, int B, int mode) {
+// want_rsm: -1 automatic (shared-memory ring slices when one sample fits),
+// 0 global ring, 1 shared-memory slices (rsm false in the result when they do
+// not fit); want_wave: 0 automatic (as many samples as fit), else at most that.
+static GPlan plan_tier_g(const Graph* g, int B, int mode, int want_rsm = -1, int want_wave = 0) {
   const size_t optin = (size_t)optin_smem();
   GPlan p{false, 1, 0};
-  const int cap = std::max(1, std::min(B, kMaxWave));
-  if (mode != MODE_ATOMIC) {
+  int cap = std::max(1, std::min(B, kMaxWave));
+  if (want_wave > 0) cap = std::min(cap, want_wave);
+  if (mode != MODE_ATOMIC && want_rsm != 0) {
     int bw = 0;
     while (bw < cap && g_smem_bytes(g->BS, g->P, g->R, bw + 1, true, true) <= optin) ++bw;
     if (bw >= 1) {
@@ -1475,7 +1479,7 @@ static int tier_g_threads(const Graph* g) {
 template <int MODE, bool RSM, bool EPR>
 static int launch_tier_g(Run* r, const FwdArgs& a, size_t smem, cudaStream_t st) {
   const Graph* g = r->g;
-  const int nthr = tier_g_threads(g);
+  const int nthr = r->cfg_threads > 0 ? r->cfg_threads : tier_g_threads(g);
   SNCB_CUDA(cudaFuncSetAttribute(k_tier_g<MODE, RSM, EPR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   SNCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tier_g<MODE, RSM, EPR>, nthr, smem));
@@ -1527,7 +1531,29 @@ static bool tier_s_fits(const Graph* g, int mode) {
 
 static bool use_tier_s(const Run* r, int mode, int path) {
   return path == SNC_B200_PATH_PERSISTENT && tier_s_fits(r->g, mode) &&
-         !(r->flags & SNC_B200_RUN_FORCE_GRID);
+         !(r->flags & SNC_B200_RUN_FORCE_GRID) && r->cfg_tier != 1;
+}
+
+int check_shape(const Run* r, int mode, int tier, int threads, int wave, int rsm) {
+  const Graph* g = r->g;
+  if (tier == 0 && !tier_s_fits(g, mode)) {
+    set_error("launch shape: one sample's state does not fit one CTA (tier 0)");
+    return SNC_B200_EUNSUPPORTED;
+  }
+  if (tier < -1 || tier > 1 || wave < 0 || rsm < -1 || rsm > 1 ||
+      (threads != 0 && (threads % 32 != 0 || threads < kGThreads || threads > kGThreadsMax))) {
+    set_error("launch shape: tier -1..1, threads 0 or a multiple of 32 in [512, 768], wave >= 0, "
+              "ring_smem -1..1");
+    return SNC_B200_EUNSUPPORTED;
+  }
+  if (rsm == 1 && mode != MODE_ATOMIC) {
+    const GPlan p = plan_tier_g(g, std::max(1, r->in->B), mode, 1, wave);
+    if (!p.rsm) {
+      set_error("launch shape: ring slices do not fit in shared memory");
+      return SNC_B200_EUNSUPPORTED;
+    }
+  }
+  return SNC_B200_OK;
 }
 
 // Launch body without timing / graph handling.
@@ -1560,11 +1586,17 @@ int launch_run(Run* r, const snc_lif* lif, int mode, int path, cudaStream_t st) 
   const Graph* g = r->g;
   const Inputs* in = r->in;
   if (mode == SNC_B200_MODE_AUTO || path == SNC_B200_PATH_AUTO) {
-    int m = mode, p = path;
-    int rc = resolve_auto(g, in, &m, &p);
+    int m = mode, p = path, shape[4] = {-1, 0, 0, -1};
+    int rc = resolve_auto(g, in, &m, &p, shape);
     if (rc) return rc;
     if (mode == SNC_B200_MODE_AUTO) mode = m;
     if (path == SNC_B200_PATH_AUTO) path = p;
+    if (!r->cfg_explicit) {  // the tuned shape, unless the caller set one
+      r->cfg_tier = shape[0];
+      r->cfg_threads = shape[1];
+      r->cfg_wave = shape[2];
+      r->cfg_rsm = shape[3];
+    }
   }
   if (mode < 0 || mode > MODE_SORT || path < 0 || path > SNC_B200_PATH_PERSISTENT) {
     set_error("bad mode or path");
@@ -1574,7 +1606,7 @@ int launch_run(Run* r, const snc_lif* lif, int mode, int path, cudaStream_t st) 
   if (!use_tier_s(r, mode, path)) {
     int Bw = 1;
     if (path == SNC_B200_PATH_PERSISTENT) {
-      const GPlan p = plan_tier_g(g, in->B, mode);
+      const GPlan p = plan_tier_g(g, in->B, mode, r->cfg_rsm, r->cfg_wave);
       Bw = p.Bw;
       r->gplan_rsm = p.rsm;
       r->gplan_smem = p.smem;
@@ -1609,8 +1641,10 @@ int launch_run(Run* r, const snc_lif* lif, int mode, int path, cudaStream_t st) 
     bool use_graph = (r->flags & SNC_B200_RUN_GRAPH) && path == SNC_B200_PATH_PERSISTENT &&
                      !r->graph_refused && a.stall == 0;
     if (use_graph) {
+      const int shape[4] = {r->cfg_tier, r->cfg_threads, r->cfg_wave, r->cfg_rsm};
       const bool same = r->gexec && r->gexec_mode == mode && r->gexec_stream == st &&
                         r->gexec_wait_ns == a.wait_ns &&
+                        std::memcmp(r->gexec_shape, shape, sizeof(shape)) == 0 &&
                         std::memcmp(&r->gexec_lif, lif, sizeof(snc_lif)) == 0;
       if (!same) {
         if (r->gexec) cudaGraphExecDestroy(r->gexec);
@@ -1638,6 +1672,7 @@ int launch_run(Run* r, const snc_lif* lif, int mode, int path, cudaStream_t st) 
           r->gexec_lif = *lif;
           r->gexec_stream = st;
           r->gexec_wait_ns = a.wait_ns;
+          std::memcpy(r->gexec_shape, shape, sizeof(shape));
         }
       }
     }

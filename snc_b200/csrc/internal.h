@@ -92,7 +92,8 @@ struct Graph {
   // targeting b) descriptors per step, stored from ibase[b].
   int G = 0;
   int* ibase = nullptr;     // [P+1]
-  long long signature = 0;  // autotuner cache key
+  long long signature = 0;  // coarse shape class (log sizes, fan-in skew, ring length)
+  unsigned long long hash = 0;  // content hash of the graph: the autotuner's cache key
   float fanin_cv = 0.f, density = 0.f;
   mutable OneShot* oneshot = nullptr;  // workspace of the one-call forwards
 };
@@ -190,6 +191,11 @@ struct Run {
   snc_lif gexec_lif{};
   cudaStream_t gexec_stream = nullptr;
   unsigned long long gexec_wait_ns = 0;  // wait bound baked into the graph
+  int gexec_shape[4] = {-1, -1, -1, -1};  // launch shape baked into the graph
+  // launch shape set by snc_b200_run_configure or an autotuned AUTO launch
+  // (tier -1 / threads 0 / wave 0 / ring_smem -1: chosen automatically)
+  int cfg_tier = -1, cfg_threads = 0, cfg_wave = 0, cfg_rsm = -1;
+  bool cfg_explicit = false;  // set by the caller: AUTO launches keep it
   cudaStream_t own_stream = nullptr;  // stands in for the legacy default stream
   bool graph_refused = false;         // stream capture failed once; launch directly
   bool used_graph = false;            // the last launch went through the graph
@@ -272,7 +278,14 @@ void free_run(Run* r);
 int launch_eprop_forward(const EpropLaunch& e, cudaStream_t stream);
 int launch_run(Run* r, const snc_lif* lif, int mode, int path, cudaStream_t stream);
 int tier_s_smem_bytes(const Graph* g, int mode, bool eprop);
-int resolve_auto(const Graph* g, const Inputs* in, int* mode, int* path);
+// AUTO resolution: the autotuned choice cached for this graph and batch (mode,
+// path and launch shape: shape[4] = tier, threads, wave, ring_smem), else a
+// default rule (shape automatic).
+int resolve_auto(const Graph* g, const Inputs* in, int* mode, int* path, int* shape);
+// Checks a launch shape for this run's graph and inputs (tier G threads a
+// multiple of 32 in [512, 768], wave within the batch and shared memory,
+// ring slices that fit).  Returns SNC_B200_OK or SNC_B200_EUNSUPPORTED.
+int check_shape(const Run* r, int mode, int tier, int threads, int wave, int rsm);
 
 }  // namespace sncb
 

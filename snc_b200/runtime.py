@@ -215,6 +215,14 @@ class Run:
         check(lib().snc_b200_run_launch(self.h, C.byref(lf), int(mode), int(path),
                                         C.c_void_p(stream) if stream else None), "run_launch")
 
+    def configure(self, tier=-1, block_threads=0, wave=0, ring_smem=-1, mode=MODE_SORT):
+        """Fix the launch shape (snc_b200_run_configure); configure(None)
+        semantics: call with no arguments to return to automatic shapes."""
+        c = _lib.LaunchConfig(int(mode), PATH_PERSISTENT, int(tier), int(block_threads), int(wave),
+                              int(ring_smem), 0.0)
+        auto = tier == -1 and block_threads == 0 and wave == 0 and ring_smem == -1
+        check(lib().snc_b200_run_configure(self.h, None if auto else C.byref(c)), "run_configure")
+
     def used(self):
         m, p = C.c_int(), C.c_int()
         check(lib().snc_b200_run_used(self.h, C.byref(m), C.byref(p)))
@@ -283,11 +291,28 @@ def forward_batched(dg: DeviceGraph, events, steps, lif: LIFParams, mode=MODE_SO
     return {"logits": logits[:, :dg.n_out], "spikes": spikes, "events": evs, "ms": st.ms}
 
 
+def _shape_dict(c) -> dict:
+    return {"mode": c.mode, "path": c.path, "tier": c.tier, "block_threads": c.block_threads,
+            "wave": c.wave, "ring_smem": c.ring_smem, "ms": c.ms}
+
+
 def autotune(dg: DeviceGraph, inputs: DeviceInputs, lif: LIFParams) -> dict:
-    """Time every delivery mode and path on this graph; the winner is cached
-    per graph signature and used by later MODE_AUTO / PATH_AUTO launches."""
-    m, p, bt = C.c_int(), C.c_int(), C.c_int()
+    """Time every launch candidate (delivery mode x path x launch shape) on
+    this graph and inputs; the winner is cached under the graph's content hash
+    and the batch's shape and used by later MODE_AUTO / PATH_AUTO launches.
+    Returns the winner (mode, path, tier, block_threads, wave, ring_smem, ms)
+    with the list of timed candidates under "candidates"."""
+    cands = (_lib.LaunchConfig * 64)()
+    n, best = C.c_int32(), C.c_int32()
     lf = lif.c()
-    check(lib().snc_b200_autotune(dg.h, inputs.h, C.byref(lf), C.byref(m), C.byref(p),
-                                  C.byref(bt)), "autotune")
-    return {"mode": m.value, "path": p.value, "block_threads": bt.value}
+    check(lib().snc_b200_autotune_ex(dg.h, inputs.h, C.byref(lf), cands, 64, C.byref(n),
+                                     C.byref(best)), "autotune")
+    out = _shape_dict(cands[best.value])
+    out["candidates"] = [_shape_dict(cands[i]) for i in range(min(64, n.value))]
+    return out
+
+
+def autotune_lookup(dg: DeviceGraph, inputs: DeviceInputs) -> dict | None:
+    """The cached autotuner choice for this graph and batch shape, or None."""
+    c = _lib.LaunchConfig()
+    return _shape_dict(c) if lib().snc_b200_autotune_lookup(dg.h, inputs.h, C.byref(c)) == 1 else None

@@ -16,14 +16,15 @@ pytestmark = pytest.mark.gpu
 BUILD = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "snc_b200",
                      "adapter", "_build")
 BENCH = os.path.join(BUILD, "snc_bench")
+BENCH_SIDE = os.path.join(BUILD, "snc_bench_side")
 TRAIN = os.path.join(BUILD, "snc_train")
 COTRAIN = os.path.join(BUILD, "snc_cotrain")
 
 
-def compare(args):
-    if not os.path.exists(BENCH):
+def compare(args, binary=BENCH):
+    if not os.path.exists(binary):
         pytest.skip("reference CLIs not built")
-    out = subprocess.run([BENCH] + args + ["--compare-backends"], capture_output=True, text=True,
+    out = subprocess.run([binary] + args + ["--compare-backends"], capture_output=True, text=True,
                          timeout=600)
     assert out.returncode == 0, out.stderr
     rows = {}
@@ -52,6 +53,29 @@ def test_snc_bench_compare_backends(args):
         assert "fallback" not in note, text
         assert match in ("exact", "approx"), text
     sp, ev, match, _ = rows["cuda-sort"][0]
+    assert (sp, ev, match) == (cpu[0], cpu[1], "exact"), text
+
+
+@pytest.mark.parametrize("args", [
+    ["--structure", "static-snc", "--encoder", "poisson", "--num-steps", "50", "--num-samples", "64",
+     "--hidden", "256"],
+    ["--structure", "random-sparse", "--num-steps", "100", "--num-samples", "16", "--hidden", "512",
+     "--synapse-budget", "200000", "--inhib", "0.5", "--decay", "0.95", "--delay", "3"],
+])
+def test_b200_backends_beside_the_reference_cuda_backend(args):
+    """The reference's backend table extended with b200-* names (beside.py),
+    its own cuda_backend.cu linked unchanged: one --compare-backends run has
+    the reference's cuda-* rows computed by its own kernels and the b200-*
+    rows by this backend, none falling back; b200-sort matches cpu exactly."""
+    rows, text = compare(args, BENCH_SIDE)
+    cpu = rows["cpu"][0]
+    for name in ("openmp", "cuda-atomic", "cuda-bucket", "cuda-sort", "b200-atomic", "b200-bucket",
+                 "b200-sort"):
+        assert name in rows, text
+        sp, ev, match, note = rows[name][0]
+        assert "fallback" not in note, text
+        assert match in ("exact", "approx"), text
+    sp, ev, match, _ = rows["b200-sort"][0]
     assert (sp, ev, match) == (cpu[0], cpu[1], "exact"), text
 
 

@@ -264,3 +264,56 @@ def test_audio700_all_256_samples_atomic(audio700_all):
     g, ev, steps, lif, ref = audio700_all
     out = run_gpu(g, ev, steps, lif, R.MODE_ATOMIC, R.PATH_PERSISTENT, cuda_graph=True)
     assert spike_count_agreement(out["spikes"], ref["spikes"]) >= 0.999
+
+
+# ---- launch shapes and the autotuner ----------------------------------------
+
+@pytest.mark.parametrize("shape", [dict(tier=0), dict(tier=1, block_threads=512, wave=1, ring_smem=1),
+                                   dict(tier=1, block_threads=768, wave=2, ring_smem=0),
+                                   dict(tier=1, block_threads=512, wave=0, ring_smem=0),
+                                   dict(tier=1, block_threads=768, wave=3, ring_smem=1)])
+@pytest.mark.parametrize("mode", [R.MODE_SORT, R.MODE_BUCKET, R.MODE_ATOMIC])
+def test_every_launch_shape_keeps_the_results(shape, mode):
+    g = W.random_graph(8, n_hid=400, max_delay=9)
+    ev, steps = W.random_events(19, g, 5, [40, 12, 33, 0, 25])
+    lif = R.LIFParams(threshold=1.0, decay=0.9, reset=0.0, refractory=1)
+    ref = O.forward_batched(g, ev, steps, lif)
+    dg = R.DeviceGraph(g)
+    di = R.DeviceInputs(dg, ev, steps)
+    run = R.Run(dg, di, raster=True, vfinal=True)
+    run.configure(mode=mode, **shape)
+    run.launch(lif, mode=mode, path=R.PATH_PERSISTENT)
+    out = run.fetch(raster=True, vfinal=True)
+    if mode == R.MODE_SORT:
+        assert_exact(out, ref)
+    else:
+        assert spike_count_agreement(out["spikes"], ref["spikes"]) >= 0.999
+
+
+def test_autotuner_times_launch_shapes_and_keys_on_the_graph():
+    """The tuner times real launch shapes (tier-1 block sizes and ring
+    placements beside the modes and paths), picks the fastest, AUTO launches
+    use it, and a second graph of the same size but other contents is not
+    covered by the first graph's entry."""
+    lif = W.lif_tau20()
+    g1 = W.rec100k_graph(seed=1, n=20000, width=200, out_degree=40)
+    g2 = W.rec100k_graph(seed=2, n=20000, width=200, out_degree=40)
+    assert (g1.num_neurons, g1.num_synapses) == (g2.num_neurons, g2.num_synapses)
+    ev1, steps = W.rec100k_inputs(g1, 1, 300, seed=1)
+    ev2, _ = W.rec100k_inputs(g2, 1, 300, seed=1)
+    dg1, dg2 = R.DeviceGraph(g1), R.DeviceGraph(g2)
+    di1, di2 = R.DeviceInputs(dg1, ev1, steps), R.DeviceInputs(dg2, ev2, steps)
+    tuned = R.autotune(dg1, di1, lif)
+    cands = tuned["candidates"]
+    tier1 = [c for c in cands if c["path"] == R.PATH_PERSISTENT and c["tier"] == 1]
+    assert len({c["block_threads"] for c in tier1}) >= 2
+    assert {c["ring_smem"] for c in tier1 if c["mode"] != R.MODE_ATOMIC} == {0, 1}
+    assert any(c["path"] == R.PATH_PLAIN for c in cands)
+    assert len({c["ms"] for c in cands}) > 1
+    assert tuned["ms"] == min(c["ms"] for c in cands)
+    assert R.autotune_lookup(dg1, di1) == {k: v for k, v in tuned.items() if k != "candidates"}
+    assert R.autotune_lookup(dg2, di2) is None
+    run = R.Run(dg1, di1)
+    run.launch(lif, mode=R.MODE_AUTO, path=R.PATH_AUTO)
+    run.fetch()
+    assert run.used() == (tuned["mode"], tuned["path"])
