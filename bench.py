@@ -244,7 +244,8 @@ def config_legs(reps=3):
     C1 (ff784: 784-256-10, 64 samples x 50 steps) and C3 (audio700: 700 input
     channels, 1024 recurrent, 20 outputs, 256 samples of 50-1000 steps) on the
     persistent and the plain path in ATOMIC and SORT delivery (device time,
-    best of `reps`), and one C3 e-prop minibatch (32 samples, the graph's
+    best of `reps`; C3's 20 outputs are leaky readout units with decay 0.9,
+    the persistent launches go through a CUDA graph), and one C3 e-prop minibatch (32 samples, the graph's
     weights, forward with eligibility + weight update, SORT) beside the CPU
     restatement of the same minibatch (one core) with the largest weight
     difference between them."""
@@ -261,6 +262,8 @@ def config_legs(reps=3):
         dg = R.DeviceGraph(g)
         di = R.DeviceInputs(dg, ev, steps)
         run = R.Run(dg, di, cuda_graph=True)  # the persistent launch goes through a CUDA graph
+        if name.startswith("C3"):
+            run.set_readout(0.9)  # C3's 20 leaky readout units
         ss = int(np.sum(steps))
         leg = {"samples": int(len(steps)), "sample_steps": ss}
         for m in (R.MODE_ATOMIC, R.MODE_SORT):

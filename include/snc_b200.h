@@ -219,6 +219,15 @@ int snc_b200_run_launch(snc_b200_run* r, const snc_lif* lif, int mode, int path,
  *   last launch). */
 int snc_b200_run_fetch(snc_b200_run* r, float* logits, int64_t* spikes, int64_t* events,
                        uint32_t* raster, float* v_final, snc_run_stats* stats);
+/* Leaky readout units (the readout of python/snc/shd_model.py:139-140,147
+ * on the substrate): with ro_decay >= 0 every OUTPUT neuron that has a
+ * channel stops spiking and integrates v = ro_decay * v + drive + delivered
+ * input (each product and sum rounded separately), and run_fetch's logits
+ * become, per channel, the sum over its readout units in ascending id of
+ * their potential after the sample's last step divided by its step count.
+ * ro_decay < 0 turns them off (spike-count logits, the default).  Applies to
+ * this run's following launches on every path. */
+int snc_b200_run_set_readout(snc_b200_run* r, float ro_decay);
 /* The mode and path the last launch actually used (after AUTO resolution). */
 int snc_b200_run_used(const snc_b200_run* r, int* mode, int* path);
 /* 1 when the last launch went through the captured CUDA graph, 0 when it was

@@ -86,8 +86,10 @@ def forward(g: SNNGraph, events, num_steps, lif, sample=-1):
             "raster": raster, "v": v}
 
 
-def forward_batched(g: SNNGraph, events, steps, lif):
-    """Per-sample run_cpu with per-sample step counts; events carry sample_id."""
+def forward_batched(g: SNNGraph, events, steps, lif, ro_decay=None):
+    """Per-sample run_cpu with per-sample step counts; events carry sample_id.
+    ro_decay: OUTPUT neurons with a channel are leaky readout units (logits =
+    their final potential / T)."""
     events = np.ascontiguousarray(events, dtype=EVENT_DTYPE)
     steps = np.ascontiguousarray(steps, dtype=np.int32)
     B = steps.shape[0]
@@ -99,9 +101,11 @@ def forward_batched(g: SNNGraph, events, steps, lif):
     evs = np.zeros(B, np.int64)
     raster = np.zeros((int(steps.sum()), W), np.uint32)
     v = np.zeros((B, g.num_neurons), np.float32)
-    rc = lib().orc_forward_batched(C.byref(gs), _ptr(events), C.c_size_t(events.shape[0]), B,
-                                   _ptr(steps), C.byref(lf), _ptr(logits), _ptr(spikes),
-                                   _ptr(evs), _ptr(raster), _ptr(v))
+    f = lib().orc_forward_batched_ro
+    f.argtypes = None
+    rc = f(C.byref(gs), _ptr(events), C.c_size_t(events.shape[0]), B, _ptr(steps), C.byref(lf),
+           C.c_float(-1.0 if ro_decay is None else float(ro_decay)), _ptr(logits), _ptr(spikes),
+           _ptr(evs), _ptr(raster), _ptr(v))
     if rc:
         raise RuntimeError(f"orc_forward_batched failed: {rc}")
     return {"logits": logits[:, :g.num_output_channels], "spikes": spikes, "events": evs,

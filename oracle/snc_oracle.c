@@ -194,9 +194,22 @@ long long orc_schedule_merged(const orc_graph* g, const orc_event* ev, size_t n_
  *  raster   [T][ceil(N/32)] bit j of word (t, i/32) set when neuron i fired at t
  *  v_out    [N]             membrane potential after the last step
  * raster / v_out may be NULL. */
+/* ro_decay >= 0: OUTPUT neurons with a channel are leaky readout units
+ * (python/snc/shd_model.py:139-140,147 on the substrate): v = v * ro_decay +
+ * ext + slot, never firing; logits[channel] = sum, ascending id, of v / T. */
+static int forward_ro(const orc_graph* g, const orc_event* ev, size_t n_ev, int sample, int T,
+                      const orc_lif* lif, float ro_decay, float* logits, int64_t* spikes_out,
+                      int64_t* events_out, uint32_t* raster, float* v_out);
+
 int orc_forward(const orc_graph* g, const orc_event* ev, size_t n_ev, int sample,
                 int T, const orc_lif* lif, float* logits, int64_t* spikes_out,
                 int64_t* events_out, uint32_t* raster, float* v_out) {
+  return forward_ro(g, ev, n_ev, sample, T, lif, -1.0f, logits, spikes_out, events_out, raster, v_out);
+}
+
+static int forward_ro(const orc_graph* g, const orc_event* ev, size_t n_ev, int sample, int T,
+                      const orc_lif* lif, float ro_decay, float* logits, int64_t* spikes_out,
+                      int64_t* events_out, uint32_t* raster, float* v_out) {
   const int n = g->num_neurons;
   int nic, noc;
   io_counts(g, &nic, &noc);
@@ -230,7 +243,9 @@ int orc_forward(const orc_graph* g, const orc_event* ev, size_t n_ev, int sample
     /* cpu_backend.cpp:129-143 -- integrate / fire / reset / refractory */
     int nf = 0;
     for (int i = 0; i < n; ++i) {
-      if (refr[i] > 0) {
+      if (ro_decay >= 0.0f && g->role[i] == 2 && g->channel[i] >= 0) {
+        v[i] = v[i] * ro_decay + ext[i] + slot[i];
+      } else if (refr[i] > 0) {
         --refr[i];
         v[i] = lif->reset;
       } else {
@@ -262,6 +277,9 @@ int orc_forward(const orc_graph* g, const orc_event* ev, size_t n_ev, int sample
       }
     }
   }
+  if (ro_decay >= 0.0f && logits)
+    for (int i = 0; i < n; ++i)
+      if (g->role[i] == 2 && g->channel[i] >= 0) logits[g->channel[i]] += v[i] / (float)T;
   if (v_out) memcpy(v_out, v, sizeof(float) * (size_t)n);
   if (spikes_out) *spikes_out = spikes;
   if (events_out) *events_out = syn_events;
@@ -274,16 +292,30 @@ int orc_forward(const orc_graph* g, const orc_event* ev, size_t n_ev, int sample
  * (events carry sample_id, include/snc/encoders.hpp:22).  Outputs are
  * concatenated per sample: logits [B][noc], spikes/events [B], raster
  * [sum_b T_b][W] (sample-major), v_out [B][N]. */
+int orc_forward_batched_ro(const orc_graph* g, const orc_event* ev, size_t n_ev,
+                           int num_samples, const int32_t* steps, const orc_lif* lif,
+                           float ro_decay, float* logits, int64_t* spikes, int64_t* events,
+                           uint32_t* raster, float* v_out);
+
 int orc_forward_batched(const orc_graph* g, const orc_event* ev, size_t n_ev,
                         int num_samples, const int32_t* steps, const orc_lif* lif,
                         float* logits, int64_t* spikes, int64_t* events,
                         uint32_t* raster, float* v_out) {
+  return orc_forward_batched_ro(g, ev, n_ev, num_samples, steps, lif, -1.0f, logits, spikes, events,
+                                raster, v_out);
+}
+
+/* orc_forward_batched with leaky readout units (ro_decay >= 0). */
+int orc_forward_batched_ro(const orc_graph* g, const orc_event* ev, size_t n_ev,
+                           int num_samples, const int32_t* steps, const orc_lif* lif,
+                           float ro_decay, float* logits, int64_t* spikes, int64_t* events,
+                           uint32_t* raster, float* v_out) {
   int nic, noc;
   io_counts(g, &nic, &noc);
   const int W = (g->num_neurons + 31) / 32;
   size_t roff = 0;
   for (int b = 0; b < num_samples; ++b) {
-    int rc = orc_forward(g, ev, n_ev, b, steps[b], lif,
+    int rc = forward_ro(g, ev, n_ev, b, steps[b], lif, ro_decay,
                          logits ? logits + (size_t)b * noc : NULL,
                          spikes ? spikes + b : NULL, events ? events + b : NULL,
                          raster ? raster + roff : NULL,

@@ -84,6 +84,7 @@ SIGNATURES = {
     "snc_b200_autotune_ex": (C.c_int, [P, P, P, P, I32, P, P]),
     "snc_b200_autotune_lookup": (C.c_int, [P, P, P]),
     "snc_b200_run_configure": (C.c_int, [P, P]),
+    "snc_b200_run_set_readout": (C.c_int, [P, C.c_float]),
     "snc_b200_eprop_create": (C.c_int, [P, P, P, I32, P, P, P]),
     "snc_b200_eprop_release": (C.c_int, [P]),
     "snc_b200_eprop_path": (C.c_int, [P]),

@@ -105,7 +105,7 @@ static void free_graph(Graph* g) {
   for (void* p : {(void*)g->row_ptr, (void*)g->edges, (void*)g->post, (void*)g->col_of,
                   (void*)g->out_ch, (void*)g->role, (void*)g->channel, (void*)g->colbase,
                   (void*)g->gedges, (void*)g->gptr, (void*)g->groups, (void*)g->ibase,
-                  (void*)g->chan_ptr, (void*)g->chan_ids})
+                  (void*)g->chan_ptr, (void*)g->chan_ids, (void*)g->ro_rank, (void*)g->ro_chan})
     dev_free(p);
 }
 
@@ -219,12 +219,23 @@ static int upload_graph(const snc_graph_view* v, Graph* g) {
   }
   std::vector<uint8_t> role(v->role, v->role + n);
   std::vector<int> channel(v->channel, v->channel + n);
+  // leaky readout units: the OUTPUT neurons with a channel, ascending id
+  std::vector<int> ro_rank(n, -1), ro_chan;
+  for (int i = 0; i < n; ++i)
+    if (out_ch[i] >= 0) {
+      ro_rank[i] = (int)ro_chan.size();
+      ro_chan.push_back(out_ch[i]);
+    }
+  g->n_ro = (int)ro_chan.size();
   // packed and destination-grouped edges, groups, inbox bases: on the device
   if ((rc = build_graph_device(v, g))) return rc;
   if ((rc = dev_upload(&g->out_ch, out_ch.data(), (size_t)n))) return rc;
   if ((rc = dev_upload(&g->role, role.data(), role.size()))) return rc;
   if ((rc = dev_upload(&g->channel, channel.data(), channel.size()))) return rc;
   if ((rc = dev_upload(&g->colbase, colbase.data(), colbase.size()))) return rc;
+  if ((rc = dev_upload(&g->ro_rank, ro_rank.data(), ro_rank.size()))) return rc;
+  if ((rc = dev_upload(&g->ro_chan, ro_chan.empty() ? nullptr : ro_chan.data(), ro_chan.size())))
+    return rc;
   if ((rc = dev_upload(&g->chan_ptr, g->chan_ptr_h.data(), g->chan_ptr_h.size()))) return rc;
   if ((rc = dev_upload(&g->chan_ids, g->chan_ids_h.empty() ? nullptr : g->chan_ids_h.data(),
                        g->chan_ids_h.size())))
@@ -243,7 +254,7 @@ void free_run(Run* r) {
   for (void* p : {(void*)r->counts, (void*)r->spikes, (void*)r->events, (void*)r->raster,
                   (void*)r->vfinal, (void*)r->err, (void*)r->ctl, (void*)r->v, (void*)r->refr,
                   (void*)r->ring, (void*)r->fired, (void*)r->fired_cnt, (void*)r->inbox,
-                  (void*)r->inbox_cnt})
+                  (void*)r->inbox_cnt, (void*)r->ro_v, (void*)r->ro_logits})
     dev_free(p);
   if (r->ev0) cudaEventDestroy(r->ev0);
   if (r->ev1) cudaEventDestroy(r->ev1);
@@ -289,9 +300,16 @@ int fetch_run(Run* r, float* logits, int64_t* spikes, int64_t* events, uint32_t*
     SNCB_CUDA(cudaMemcpy(sp.data(), r->spikes, (size_t)B * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
     SNCB_CUDA(cudaMemcpy(evn.data(), r->events, (size_t)B * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   }
-  if (logits)
+  if (logits && r->ro_decay >= 0.f && r->ro_logits && B > 0) {
+    // leaky readout units: their potentials over the sample's steps
+    std::vector<float> lg((size_t)B * noc);
+    SNCB_CUDA(cudaMemcpy(lg.data(), r->ro_logits, lg.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    for (int b = 0; b < B; ++b)
+      for (int c = 0; c < g->noc; ++c) logits[(size_t)b * g->noc + c] = lg[(size_t)b * noc + c];
+  } else if (logits) {
     for (int b = 0; b < B; ++b)
       for (int c = 0; c < g->noc; ++c) logits[(size_t)b * g->noc + c] = (float)counts[(size_t)b * noc + c];
+  }
   long long ts = 0, te = 0;
   for (int b = 0; b < B; ++b) {
     if (spikes) spikes[b] = (int64_t)sp[b];
@@ -563,6 +581,21 @@ int snc_b200_forward_batched(const snc_b200_graph* graph, const snc_input_event*
   if (!graph || !lif) { set_error("null argument"); return SNC_B200_EINVAL; }
   return oneshot_forward(graph, events, n_events, num_samples, steps, false, lif, mode,
                          SNC_B200_PATH_PERSISTENT, logits, spikes, events_out, stats);
+}
+
+int snc_b200_run_set_readout(snc_b200_run* r, float ro_decay) {
+  if (!r) { set_error("null run"); return SNC_B200_EINVAL; }
+  if (!(ro_decay >= 0.f)) {  // off (negative or NaN)
+    r->ro_decay = -1.f;
+    return SNC_B200_OK;
+  }
+  const Graph* g = r->g;
+  const size_t B = (size_t)std::max(1, r->in->B);
+  int rc;
+  if (!r->ro_v && (rc = dev_alloc(&r->ro_v, B * std::max(1, g->n_ro)))) return rc;
+  if (!r->ro_logits && (rc = dev_alloc(&r->ro_logits, B * std::max(1, g->noc)))) return rc;
+  r->ro_decay = ro_decay;
+  return SNC_B200_OK;
 }
 
 int snc_b200_run_configure(snc_b200_run* r, const snc_launch_config* cfg) {

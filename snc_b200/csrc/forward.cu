@@ -108,6 +108,16 @@ struct FwdArgs {
   // block makes (a stall injected for failure tests: every wait runs out)
   unsigned long long wait_ns;
   unsigned stall;
+  // leaky readout units (ro_on): OUTPUT neurons integrate v = ro_decay * v +
+  // drive + ring and never fire; each sample's final potentials go to
+  // ro_v [B][n_ro] at their rank, k_readout_logits turns them into logits
+  int ro_on;
+  float ro_decay;
+  const int* ro_rank;
+  const int* ro_chan;
+  int n_ro;
+  float* ro_v;
+  float* ro_logits;
 };
 
 // Shared-memory bytes of the tier-S kernel for this graph.
@@ -148,6 +158,32 @@ __device__ __forceinline__ int lif_step(const LifP& p, float& v, int& refr, floa
   }
   v = nv;
   return 0;
+}
+
+// A leaky readout unit (shd_model.py:139-140 with the substrate's delivered
+// current as its input): v = ro_decay * v + ext + ring, rounded like the LIF
+// integration; it never fires or resets.
+__device__ __forceinline__ int readout_step(float ro_decay, float& v, float ext, float rin,
+                                            float* vpre = nullptr) {
+  v = lif_integrate(v, ro_decay, ext, rin);
+  if (vpre) *vpre = v;
+  return 0;
+}
+
+// logits[b][c] = sum over the readout units of channel c, ascending id, of
+// their final potential / T_b (shd_model.py:147 averages the readout over
+// the steps).  One block per sample, a thread per channel.
+__global__ void k_readout_logits(const float* __restrict__ ro_v, const int* __restrict__ ro_chan,
+                                 int n_ro, const int* __restrict__ steps, int noc,
+                                 float* __restrict__ logits) {
+  const int b = blockIdx.x;
+  const float T = (float)max(1, steps[b]);
+  for (int c = threadIdx.x; c < noc; c += blockDim.x) {
+    float acc = 0.f;
+    for (int r = 0; r < n_ro; ++r)
+      if (ro_chan[r] == c) acc = __fadd_rn(acc, __fdiv_rn(ro_v[(size_t)b * n_ro + r], T));
+    logits[(size_t)b * noc + c] = acc;
+  }
 }
 
 // Ring slot of a delivery made at step slot `s0` with delay d (1 <= d < R).
@@ -488,7 +524,9 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
             slot[c] = 0.f;
           }
           float vpre;
-          f = lif_step(a.lif, vv, rr, e, rin, &vpre);
+          const int oc = a.out_ch[j];
+          f = a.ro_on && oc >= 0 ? readout_step(a.ro_decay, vv, e, rin, &vpre)
+                                 : lif_step(a.lif, vv, rr, e, rin, &vpre);
           v[j] = vv;
           refr[j] = rr;
           if (EP) {
@@ -507,7 +545,6 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
           if (f) {
             ++my_spikes;
             my_events += a.row_ptr[j + 1] - a.row_ptr[j];
-            const int oc = a.out_ch[j];
             if (oc >= 0) atomicAdd(&counts[oc], 1);
           }
         }
@@ -629,6 +666,9 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
     for (int i = tid; i < noc; i += nthr) a.counts[(size_t)b * noc + i] = counts[i];
     if (a.vfinal)
       for (int i = tid; i < N; i += nthr) a.vfinal[(size_t)b * N + i] = v[i];
+    if (a.ro_on)
+      for (int i = tid; i < N; i += nthr)
+        if (a.ro_rank[i] >= 0) a.ro_v[(size_t)b * a.n_ro + a.ro_rank[i]] = v[i];
     const long long ts = block_sum_ll(my_spikes, lscratch);
     const long long te = block_sum_ll(my_events, lscratch);
     if (tid == 0) {
@@ -782,7 +822,9 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, unsigne
       const float e = ext[jj];
       ext[jj] = 0.f;
       float vpre;
-      f = lif_step(a.lif, vv, rr, e, rin, EPR ? &vpre : nullptr);
+      const int oc = PERSIST ? sm.och[jj] : a.out_ch[j];
+      f = a.ro_on && oc >= 0 ? readout_step(a.ro_decay, vv, e, rin, EPR ? &vpre : nullptr)
+                             : lif_step(a.lif, vv, rr, e, rin, EPR ? &vpre : nullptr);
       if (EPR && c >= 0) {
         // e-prop (cuda_trainer.cu:93-94): the triangular surrogate of this
         // column and step, for the deferred eligibility
@@ -807,7 +849,6 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, unsigne
           asm volatile("prefetch.global.L1 [%0];" ::"l"(gr));
           asm volatile("prefetch.global.L1 [%0];" ::"l"(a.groups + max(sm.gp[jj], sm.gp[jj + 1] - 1)));
         }
-        const int oc = PERSIST ? sm.och[jj] : a.out_ch[j];
         if (oc >= 0) atomicAdd(&a.counts[(size_t)sample * a.noc + oc], 1);
         if (EPR && a.fires) atomicAdd(&a.fires[j], 1ull);
       }
@@ -1252,6 +1293,11 @@ __global__ void __launch_bounds__(kGThreadsMax, 1) k_tier_g(FwdArgs a) {
       for (int k = 0; k < nk; ++k)
         for (int j = lo + tid; j < hi; j += nthr)
           a.vfinal[(size_t)s_samp[k] * a.N + j] = sm.v[k * BS + (j - lo)];
+    if (a.ro_on)
+      for (int k = 0; k < nk; ++k)
+        for (int j = lo + tid; j < hi; j += nthr)
+          if (sm.och[j - lo] >= 0)
+            a.ro_v[(size_t)s_samp[k] * a.n_ro + a.ro_rank[j]] = sm.v[k * BS + (j - lo)];
     target += nb;
     if (!grid_sync(&a.ctl[0], target, a.err, a.wait_ns)) return;
   }
@@ -1299,8 +1345,10 @@ __global__ void k_plain_init(FwdArgs a) {
 }
 
 __global__ void k_copy_v(FwdArgs a, int sample) {
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < a.N; j += gridDim.x * blockDim.x)
-    a.vfinal[(size_t)sample * a.N + j] = a.v[j];
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < a.N; j += gridDim.x * blockDim.x) {
+    if (a.vfinal) a.vfinal[(size_t)sample * a.N + j] = a.v[j];
+    if (a.ro_on && a.ro_rank[j] >= 0) a.ro_v[(size_t)sample * a.n_ro + a.ro_rank[j]] = a.v[j];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1334,6 +1382,13 @@ static FwdArgs make_args(Run* r, const snc_lif* lif) {
   a.psi_T = r->psi_T;
   a.fires = r->fires;
   a.gamma = r->gamma;
+  a.ro_on = r->ro_decay >= 0.f && r->ro_v && r->ro_logits ? 1 : 0;
+  a.ro_decay = a.ro_on ? r->ro_decay : 0.f;
+  a.ro_rank = g->ro_rank;
+  a.ro_chan = g->ro_chan;
+  a.n_ro = g->n_ro;
+  a.ro_v = r->ro_v;
+  a.ro_logits = r->ro_logits;
   return a;
 }
 
@@ -1518,7 +1573,8 @@ static int launch_plain(Run* r, FwdArgs a, cudaStream_t st) {
       k_plain_a<MODE><<<g->P, nthr, smem, st>>>(a, smp, gb + t, t);
       if (MODE != MODE_ATOMIC) k_plain_b<MODE><<<g->P, nthr, smem, st>>>(a, t);
     }
-    if (a.vfinal) k_copy_v<<<std::max(1, std::min(1024, (g->N + 255) / 256)), 256, 0, st>>>(a, smp);
+    if (a.vfinal || a.ro_on)
+      k_copy_v<<<std::max(1, std::min(1024, (g->N + 255) / 256)), 256, 0, st>>>(a, smp);
   }
   SNCB_CUDA(cudaGetLastError());
   return SNC_B200_OK;
@@ -1556,8 +1612,22 @@ int check_shape(const Run* r, int mode, int tier, int threads, int wave, int rsm
   return SNC_B200_OK;
 }
 
-// Launch body without timing / graph handling.
+static int launch_kernels(Run* r, const FwdArgs& a, int mode, int path, cudaStream_t st);
+
+// Launch body without timing / graph handling: the forward, then the logits
+// of the leaky readout units when they are on.
 static int launch_body(Run* r, const FwdArgs& a, int mode, int path, cudaStream_t st) {
+  int rc = launch_kernels(r, a, mode, path, st);
+  if (rc || !a.ro_on) return rc;
+  if (r->in->B > 0) {
+    k_readout_logits<<<r->in->B, 32, 0, st>>>(a.ro_v, a.ro_chan, a.n_ro, r->in->steps, a.noc,
+                                              a.ro_logits);
+    SNCB_CUDA(cudaGetLastError());
+  }
+  return SNC_B200_OK;
+}
+
+static int launch_kernels(Run* r, const FwdArgs& a, int mode, int path, cudaStream_t st) {
   if (use_tier_s(r, mode, path)) {
     if (mode == MODE_SORT) return launch_tier_s<MODE_SORT>(r, a, st);
     return launch_tier_s<MODE_ATOMIC>(r, a, st);
@@ -1643,7 +1713,7 @@ int launch_run(Run* r, const snc_lif* lif, int mode, int path, cudaStream_t st) 
     if (use_graph) {
       const int shape[4] = {r->cfg_tier, r->cfg_threads, r->cfg_wave, r->cfg_rsm};
       const bool same = r->gexec && r->gexec_mode == mode && r->gexec_stream == st &&
-                        r->gexec_wait_ns == a.wait_ns &&
+                        r->gexec_wait_ns == a.wait_ns && r->gexec_ro == (a.ro_on ? a.ro_decay : -1.f) &&
                         std::memcmp(r->gexec_shape, shape, sizeof(shape)) == 0 &&
                         std::memcmp(&r->gexec_lif, lif, sizeof(snc_lif)) == 0;
       if (!same) {
@@ -1673,6 +1743,7 @@ int launch_run(Run* r, const snc_lif* lif, int mode, int path, cudaStream_t st) 
           r->gexec_stream = st;
           r->gexec_wait_ns = a.wait_ns;
           std::memcpy(r->gexec_shape, shape, sizeof(shape));
+          r->gexec_ro = a.ro_on ? a.ro_decay : -1.f;
         }
       }
     }

@@ -92,6 +92,11 @@ struct Graph {
   // targeting b) descriptors per step, stored from ibase[b].
   int G = 0;
   int* ibase = nullptr;     // [P+1]
+  // leaky readout units (OUTPUT neurons with a channel, ascending id): rank of
+  // each neuron among them or -1, and each rank's channel
+  int n_ro = 0;
+  int* ro_rank = nullptr;   // [N]
+  int* ro_chan = nullptr;   // [n_ro]
   long long signature = 0;  // coarse shape class (log sizes, fan-in skew, ring length)
   unsigned long long hash = 0;  // content hash of the graph: the autotuner's cache key
   float fanin_cv = 0.f, density = 0.f;
@@ -196,6 +201,11 @@ struct Run {
   // (tier -1 / threads 0 / wave 0 / ring_smem -1: chosen automatically)
   int cfg_tier = -1, cfg_threads = 0, cfg_wave = 0, cfg_rsm = -1;
   bool cfg_explicit = false;  // set by the caller: AUTO launches keep it
+  // leaky readout units (snc_b200_run_set_readout): decay, or < 0 when off;
+  // final potential of every readout unit [B][n_ro] and the logits [B][noc]
+  float ro_decay = -1.f, gexec_ro = -1.f;
+  float* ro_v = nullptr;
+  float* ro_logits = nullptr;
   cudaStream_t own_stream = nullptr;  // stands in for the legacy default stream
   bool graph_refused = false;         // stream capture failed once; launch directly
   bool used_graph = false;            // the last launch went through the graph

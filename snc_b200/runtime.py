@@ -215,6 +215,11 @@ class Run:
         check(lib().snc_b200_run_launch(self.h, C.byref(lf), int(mode), int(path),
                                         C.c_void_p(stream) if stream else None), "run_launch")
 
+    def set_readout(self, ro_decay):
+        """Leaky readout units on the OUTPUT neurons (None or < 0: off)."""
+        check(lib().snc_b200_run_set_readout(self.h, -1.0 if ro_decay is None else float(ro_decay)),
+              "run_set_readout")
+
     def configure(self, tier=-1, block_threads=0, wave=0, ring_smem=-1, mode=MODE_SORT):
         """Fix the launch shape (snc_b200_run_configure); configure(None)
         semantics: call with no arguments to return to automatic shapes."""

@@ -317,3 +317,44 @@ def test_autotuner_times_launch_shapes_and_keys_on_the_graph():
     run.launch(lif, mode=R.MODE_AUTO, path=R.PATH_AUTO)
     run.fetch()
     assert run.used() == (tuned["mode"], tuned["path"])
+
+
+# ---- leaky readout units ------------------------------------------------------
+
+@pytest.mark.parametrize("pname,path,force", PATHS)
+@pytest.mark.parametrize("cuda_graph", [False, True])
+def test_leaky_readout_units_bit_exact(pname, path, force, cuda_graph):
+    """OUTPUT neurons as leaky readout units (ro_decay 0.9): logits (final
+    potential / T, per channel), rasters and potentials bit-identical to the
+    restatement on every path; switching them off restores spike counts."""
+    g = W.random_graph(9, n_hid=150, n_out=6, max_delay=8)
+    ev, steps = W.random_events(21, g, 4, [45, 0, 30, 60])
+    lif = R.LIFParams(threshold=1.0, decay=0.9, reset=0.0, refractory=1, reset_mode=1)
+    ref = O.forward_batched(g, ev, steps, lif, ro_decay=0.9)
+    dg = R.DeviceGraph(g)
+    di = R.DeviceInputs(dg, ev, steps)
+    run = R.Run(dg, di, raster=True, vfinal=True, cuda_graph=cuda_graph, force_grid=force)
+    run.set_readout(0.9)
+    for _ in range(2):
+        run.launch(lif, mode=R.MODE_SORT, path=path)
+        out = run.fetch(raster=True, vfinal=True)
+        assert_exact(out, ref)
+    assert np.abs(ref["logits"]).sum() > 0
+    run.set_readout(None)
+    run.launch(lif, mode=R.MODE_SORT, path=path)
+    assert_exact(run.fetch(raster=True, vfinal=True), O.forward_batched(g, ev, steps, lif))
+
+
+def test_audio700_all_256_samples_leaky_readout(audio700_all):
+    """C3 as configured: 20 leaky readout units (ro_decay 0.9) on all 256
+    uneven samples in one graph-launched persistent run."""
+    g, ev, steps, lif, _ = audio700_all
+    ref = O.forward_batched(g, ev, steps, lif, ro_decay=0.9)
+    dg = R.DeviceGraph(g)
+    di = R.DeviceInputs(dg, ev, steps)
+    run = R.Run(dg, di, raster=True, vfinal=True, cuda_graph=True)
+    run.set_readout(0.9)
+    run.launch(lif, mode=R.MODE_SORT, path=R.PATH_PERSISTENT)
+    out = run.fetch(raster=True, vfinal=True)
+    assert run.used_graph()
+    assert_exact(out, ref)
