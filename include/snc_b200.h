@@ -148,6 +148,14 @@ int snc_b200_inject_alloc_failure(int64_t after);
  * Limits: N < 2^24, max delay <= 255. */
 int snc_b200_graph_upload(const snc_graph_view* g, snc_b200_graph** out);
 int snc_b200_graph_release(snc_b200_graph* g);
+/* Upload a graph from the bytes of an SNCG file (the format snc_export
+ * writes, src/bench/snc_export.cpp:107-123, read by python/snc/graph.py:
+ * 11-24; pre[] in CSR order), optionally followed by the weights section
+ * 'SNCW', S, weights[S] fp32, sign[N] int32 that the reference's readers
+ * ignore (without it every weight is 1 and every sign +1).  The image is
+ * copied to the device once and its edges are checked, counted and packed
+ * there; the same validation and limits as snc_b200_graph_upload apply. */
+int snc_b200_graph_upload_sncg(const void* data, size_t bytes, snc_b200_graph** out);
 /* Basic shape: N, S, ring length, output channels, input channels. */
 int snc_b200_graph_info(const snc_b200_graph* g, int32_t* n, int32_t* s, int32_t* ring_len,
                         int32_t* n_out, int32_t* n_in);

@@ -68,6 +68,7 @@ SIGNATURES = {
     "snc_b200_inject_alloc_failure": (C.c_int, [C.c_int64]),
     "snc_b200_graph_upload": (C.c_int, [P, P]),
     "snc_b200_graph_release": (C.c_int, [P]),
+    "snc_b200_graph_upload_sncg": (C.c_int, [P, C.c_size_t, P]),
     "snc_b200_graph_info": (C.c_int, [P, P, P, P, P, P]),
     "snc_b200_graph_layout": (C.c_int, [P] * 11),
     "snc_b200_inputs_upload": (C.c_int, [P, P, C.c_size_t, I32, P, P]),

@@ -99,7 +99,7 @@ static int validate_view(const snc_graph_view* v) {
   return SNC_B200_OK;
 }
 
-static void free_graph(Graph* g) {
+void free_graph(Graph* g) {
   if (!g) return;
   free_oneshot(g);
   for (void* p : {(void*)g->row_ptr, (void*)g->edges, (void*)g->post, (void*)g->col_of,
@@ -112,7 +112,7 @@ static void free_graph(Graph* g) {
 // 64-bit content hash of a graph view (sizes and every array, weights by
 // their bits): the autotuner's cache key.  Words are folded pairwise with a
 // multiply-xorshift mix, one pass over the arrays.
-static unsigned long long graph_hash(const snc_graph_view* v) {
+unsigned long long graph_hash_view(const snc_graph_view* v) {
   unsigned long long h = 0x9E3779B97F4A7C15ull ^ ((unsigned long long)v->num_neurons << 32) ^
                          (unsigned)v->num_synapses;
   auto mix = [&h](unsigned long long x) {
@@ -143,43 +143,39 @@ static unsigned long long graph_hash(const snc_graph_view* v) {
   return h;
 }
 
-static int upload_graph(const snc_graph_view* v, Graph* g) {
-  int rc = validate_view(v);
-  if (rc) return rc;
-  g->hash = graph_hash(v);
-  const int n = v->num_neurons, m = v->num_synapses;
+// The per-neuron tables of a graph on the host (O(N) work) from its sizes,
+// largest delay, row pointers, in-degrees and per-neuron arrays, and their
+// upload; the O(S) columns are packed on the device afterwards.
+int setup_tables(Graph* g, int n, int m, int max_delay, const int32_t* row_ptr,
+                        const int* indeg, const uint8_t* role_v, const int32_t* channel_v) {
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&g->sm_count, cudaDevAttrMultiProcessorCount, dev);
   g->N = n;
   g->S = m;
-  int max_delay = 1;
-  for (int s = 0; s < m; ++s) max_delay = std::max(max_delay, v->delays[s]);
   g->max_delay = max_delay;
   g->R = max_delay + 1;
   // rebuild_io_index (snn_graph.cpp:13-28)
   int max_in = -1, max_out = -1;
   for (int i = 0; i < n; ++i) {
-    if (v->role[i] == 1) max_in = std::max(max_in, v->channel[i]);
-    else if (v->role[i] == 2) max_out = std::max(max_out, v->channel[i]);
+    if (role_v[i] == 1) max_in = std::max(max_in, channel_v[i]);
+    else if (role_v[i] == 2) max_out = std::max(max_out, channel_v[i]);
   }
   g->nic = max_in + 1;
   g->noc = max_out + 1;
   // channel -> INPUT neurons (ascending id), cpu_backend.cpp:50-55
   g->chan_ptr_h.assign(std::max(0, g->nic) + 1, 0);
   for (int i = 0; i < n; ++i)
-    if (v->role[i] == 1 && v->channel[i] >= 0 && v->channel[i] < g->nic) g->chan_ptr_h[v->channel[i] + 1]++;
+    if (role_v[i] == 1 && channel_v[i] >= 0 && channel_v[i] < g->nic) g->chan_ptr_h[channel_v[i] + 1]++;
   for (int c = 0; c < g->nic; ++c) g->chan_ptr_h[c + 1] += g->chan_ptr_h[c];
   g->chan_ids_h.assign(g->chan_ptr_h[std::max(0, g->nic)], 0);
   {
     std::vector<int> fill(std::max(0, g->nic), 0);
     for (int i = 0; i < n; ++i)
-      if (v->role[i] == 1 && v->channel[i] >= 0 && v->channel[i] < g->nic)
-        g->chan_ids_h[g->chan_ptr_h[v->channel[i]] + fill[v->channel[i]]++] = i;
+      if (role_v[i] == 1 && channel_v[i] >= 0 && channel_v[i] < g->nic)
+        g->chan_ids_h[g->chan_ptr_h[channel_v[i]] + fill[channel_v[i]]++] = i;
   }
   // ring columns for neurons with incoming synapses, ascending id
-  std::vector<int> indeg(n, 0);
-  for (int s = 0; s < m; ++s) indeg[v->post_ids[s]]++;
   g->col_of_h.assign(n, -1);
   int nc = 0;
   for (int i = 0; i < n; ++i)
@@ -187,8 +183,8 @@ static int upload_graph(const snc_graph_view* v, Graph* g) {
   g->ncols = nc;
   std::vector<int> out_ch(n, -1);
   for (int i = 0; i < n; ++i)
-    if (v->role[i] == 2 && v->channel[i] >= 0) out_ch[i] = v->channel[i];
-  g->row_ptr_h.assign(v->row_ptr, v->row_ptr + n + 1);
+    if (role_v[i] == 2 && channel_v[i] >= 0) out_ch[i] = channel_v[i];
+  g->row_ptr_h.assign(row_ptr, row_ptr + n + 1);
   // block partition for the grid kernels
   const int sm = std::max(1, g->sm_count);
   int BS = (n + sm - 1) / sm;
@@ -217,8 +213,8 @@ static int upload_graph(const snc_graph_view* v, Graph* g) {
     const long long lg = (long long)std::log2(std::max(1, n)) * 64 + (long long)std::log2(std::max(1, m));
     g->signature = (lg << 16) ^ ((long long)(g->fanin_cv * 4) << 8) ^ (long long)g->R;
   }
-  std::vector<uint8_t> role(v->role, v->role + n);
-  std::vector<int> channel(v->channel, v->channel + n);
+  std::vector<uint8_t> role(role_v, role_v + n);
+  std::vector<int> channel(channel_v, channel_v + n);
   // leaky readout units: the OUTPUT neurons with a channel, ascending id
   std::vector<int> ro_rank(n, -1), ro_chan;
   for (int i = 0; i < n; ++i)
@@ -227,8 +223,8 @@ static int upload_graph(const snc_graph_view* v, Graph* g) {
       ro_chan.push_back(out_ch[i]);
     }
   g->n_ro = (int)ro_chan.size();
-  // packed and destination-grouped edges, groups, inbox bases: on the device
-  if ((rc = build_graph_device(v, g))) return rc;
+  int rc;
+  if ((rc = dev_upload(&g->col_of, g->col_of_h.data(), (size_t)n))) return rc;
   if ((rc = dev_upload(&g->out_ch, out_ch.data(), (size_t)n))) return rc;
   if ((rc = dev_upload(&g->role, role.data(), role.size()))) return rc;
   if ((rc = dev_upload(&g->channel, channel.data(), channel.size()))) return rc;
@@ -243,6 +239,20 @@ static int upload_graph(const snc_graph_view* v, Graph* g) {
   g->max_fan = 0;
   for (int c = 0; c < g->nic; ++c) g->max_fan = std::max(g->max_fan, g->chan_ptr_h[c + 1] - g->chan_ptr_h[c]);
   return SNC_B200_OK;
+}
+
+static int upload_graph(const snc_graph_view* v, Graph* g) {
+  int rc = validate_view(v);
+  if (rc) return rc;
+  g->hash = graph_hash_view(v);
+  const int n = v->num_neurons, m = v->num_synapses;
+  int max_delay = 1;
+  for (int s = 0; s < m; ++s) max_delay = std::max(max_delay, v->delays[s]);
+  std::vector<int> indeg(n, 0);
+  for (int s = 0; s < m; ++s) indeg[v->post_ids[s]]++;
+  if ((rc = setup_tables(g, n, m, max_delay, v->row_ptr, indeg.data(), v->role, v->channel))) return rc;
+  // packed and destination-grouped edges, groups, inbox bases: on the device
+  return build_graph_device(v, g);
 }
 
 // build_schedule (cpu_backend.cpp:43-65) for a batch: per (sample, step) the

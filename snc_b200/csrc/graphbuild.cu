@@ -136,7 +136,9 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_regroup(BuildArgs a) {
 
 }  // namespace
 
-int build_graph_device(const snc_graph_view* v, Graph* g) {
+// The build proper: g->row_ptr, g->post and g->col_of are on the device;
+// w, delays and sign are device columns.
+static int build_core(Graph* g, const float* w, const int* delays, const int8_t* sign) {
   const int n = g->N, m = g->S, P = g->P;
   if (P > kMaxBlocks) {
     set_error("more neuron blocks than the device graph build handles");
@@ -145,23 +147,12 @@ int build_graph_device(const snc_graph_view* v, Graph* g) {
   DevBuf raw;
   size_t off = 0;
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-  const size_t o_w = off;     off = al(off + (size_t)std::max(1, m) * 4);
-  const size_t o_d = off;     off = al(off + (size_t)std::max(1, m) * 4);
-  const size_t o_sign = off;  off = al(off + (size_t)std::max(1, n));
   const size_t o_gc = off;    off = al(off + (size_t)std::max(1, n) * 4);
   const size_t o_ic = off;    off = al(off + (size_t)P * 4);
   const size_t o_scan = off;  off = al(off + scan_scratch_ints(std::max(n, P)) * 4);
   int rc;
   if ((rc = raw.reserve(off))) return rc;
   unsigned char* R = static_cast<unsigned char*>(raw.p);
-  if ((rc = dev_upload(&g->row_ptr, v->row_ptr, (size_t)n + 1))) return rc;
-  if ((rc = dev_upload(&g->post, v->post_ids, (size_t)m))) return rc;
-  if ((rc = dev_upload(&g->col_of, g->col_of_h.data(), (size_t)n))) return rc;
-  if (m) {
-    SNCB_CUDA(cudaMemcpy(R + o_w, v->weights, (size_t)m * 4, cudaMemcpyHostToDevice));
-    SNCB_CUDA(cudaMemcpy(R + o_d, v->delays, (size_t)m * 4, cudaMemcpyHostToDevice));
-  }
-  if (n) SNCB_CUDA(cudaMemcpy(R + o_sign, v->sign, (size_t)n, cudaMemcpyHostToDevice));
   if ((rc = dev_alloc(&g->edges, (size_t)m + 2))) return rc;
   if ((rc = dev_alloc(&g->gedges, (size_t)m + 2))) return rc;
   if ((rc = dev_alloc(&g->gptr, (size_t)n + 1))) return rc;
@@ -175,9 +166,9 @@ int build_graph_device(const snc_graph_view* v, Graph* g) {
   a.P = P;
   a.row_ptr = g->row_ptr;
   a.post = g->post;
-  a.w = reinterpret_cast<const float*>(R + o_w);
-  a.delays = reinterpret_cast<const int*>(R + o_d);
-  a.sign = reinterpret_cast<const int8_t*>(R + o_sign);
+  a.w = w;
+  a.delays = delays;
+  a.sign = sign;
   a.col_of = g->col_of;
   a.gcount = reinterpret_cast<int*>(R + o_gc);
   a.gptr = g->gptr;
@@ -204,6 +195,31 @@ int build_graph_device(const snc_graph_view* v, Graph* g) {
   if ((rc = scan_exclusive(a.icount, g->ibase, P, scan, nullptr))) return rc;
   SNCB_CUDA(cudaDeviceSynchronize());
   return SNC_B200_OK;
+}
+
+int build_graph_device(const snc_graph_view* v, Graph* g) {
+  const int n = g->N, m = g->S;
+  DevBuf cols;
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t o_w = 0;
+  const size_t o_d = al(o_w + (size_t)std::max(1, m) * 4);
+  const size_t o_sign = al(o_d + (size_t)std::max(1, m) * 4);
+  int rc;
+  if ((rc = cols.reserve(al(o_sign + (size_t)std::max(1, n))))) return rc;
+  unsigned char* C = static_cast<unsigned char*>(cols.p);
+  if ((rc = dev_upload(&g->row_ptr, v->row_ptr, (size_t)n + 1))) return rc;
+  if ((rc = dev_upload(&g->post, v->post_ids, (size_t)m))) return rc;
+  if (m) {
+    SNCB_CUDA(cudaMemcpy(C + o_w, v->weights, (size_t)m * 4, cudaMemcpyHostToDevice));
+    SNCB_CUDA(cudaMemcpy(C + o_d, v->delays, (size_t)m * 4, cudaMemcpyHostToDevice));
+  }
+  if (n) SNCB_CUDA(cudaMemcpy(C + o_sign, v->sign, (size_t)n, cudaMemcpyHostToDevice));
+  return build_core(g, reinterpret_cast<const float*>(C + o_w), reinterpret_cast<const int*>(C + o_d),
+                    reinterpret_cast<const int8_t*>(C + o_sign));
+}
+
+int build_graph_device_cols(Graph* g, const float* w, const int* delays, const int8_t* sign) {
+  return build_core(g, w, delays, sign);
 }
 
 }  // namespace sncb

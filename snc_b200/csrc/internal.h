@@ -265,7 +265,16 @@ size_t scan_scratch_ints(long long n);
 int scan_exclusive(const int* in, int* out, long long n, int* scratch, cudaStream_t st);
 // graphbuild.cu: packed and destination-grouped edges, groups and inbox
 // bases of a validated graph, built on the device (g->N, S, BS, P, col_of_h set).
+// api.cu: the per-neuron tables of a graph (O(N), host) and their upload;
+// the content hash of a graph view; release of a graph's device arrays.
+int setup_tables(Graph* g, int n, int m, int max_delay, const int32_t* row_ptr, const int* indeg,
+                 const uint8_t* role, const int32_t* channel);
+unsigned long long graph_hash_view(const snc_graph_view* v);
+void free_graph(Graph* g);
 int build_graph_device(const snc_graph_view* v, Graph* g);
+// The same from columns already on the device (g->row_ptr, g->post and
+// g->col_of set; weights, delays and per-neuron signs as device arrays).
+int build_graph_device_cols(Graph* g, const float* w, const int* delays, const int8_t* sign);
 // The schedule of a batch encoded on the device from its features.
 int encode_inputs(const Graph* g, int enc, const float* features, int C, int B, const int32_t* steps,
                   float gain, float max_rate, float threshold, uint64_t seed, Inputs* in);

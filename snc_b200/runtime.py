@@ -108,12 +108,31 @@ def _events(events) -> np.ndarray:
 class DeviceGraph:
     """A graph uploaded once (snc_b200_graph_upload)."""
 
-    def __init__(self, g: SNNGraph):
+    def __init__(self, g: SNNGraph | None, _handle=None):
         self.host = g
-        view = graph_view(g)
-        h = C.c_void_p()
-        check(lib().snc_b200_graph_upload(C.byref(view), C.byref(h)), "graph_upload")
+        if _handle is None:
+            view = graph_view(g)
+            h = C.c_void_p()
+            check(lib().snc_b200_graph_upload(C.byref(view), C.byref(h)), "graph_upload")
+        else:
+            h = _handle
         self.h = h
+        self._info()
+
+    @classmethod
+    def from_sncg(cls, data) -> "DeviceGraph":
+        """Upload an SNCG file (a path or its bytes) parsed and packed on the
+        device (snc_b200_graph_upload_sncg)."""
+        if not isinstance(data, (bytes, bytearray, memoryview)):
+            with open(data, "rb") as f:
+                data = f.read()
+        buf = (C.c_char * len(data)).from_buffer_copy(data) if not isinstance(data, bytearray) \
+            else (C.c_char * len(data)).from_buffer(data)
+        h = C.c_void_p()
+        check(lib().snc_b200_graph_upload_sncg(buf, len(data), C.byref(h)), "graph_upload_sncg")
+        return cls(None, _handle=h)
+
+    def _info(self):
         n, s, r, no, ni = (C.c_int32() for _ in range(5))
         check(lib().snc_b200_graph_info(self.h, C.byref(n), C.byref(s), C.byref(r), C.byref(no),
                                         C.byref(ni)))

@@ -99,3 +99,30 @@ def test_rec100k_shape():
     assert s["num_neurons"] == 100_000 and s["num_synapses"] == 10_000_000
     assert s["fan_in_cv"] > 0.9  # heavy-tailed in-degree
     assert g.max_delay == 30 and g.num_input_channels == 10_000
+
+
+def test_sncg_device_ingest_rejects_bad_headers_on_the_host(tmp_path):
+    """snc_b200_graph_upload_sncg checks the header, the sizes and the
+    per-neuron arrays on the host before touching a device."""
+    import ctypes as C
+    from snc_b200 import _lib
+    g = W.random_graph(2)
+    p = tmp_path / "g.sncg"
+    G.save_sncg(g, p)
+    data = bytearray(p.read_bytes())
+    L = _lib.lib()
+
+    def status(b):
+        h = C.c_void_p()
+        buf = (C.c_char * len(b)).from_buffer_copy(bytes(b))
+        return L.snc_b200_graph_upload_sncg(buf, len(b), C.byref(h))
+
+    bad = bytearray(data); bad[0] ^= 1
+    assert status(bad) == _lib.EINVAL and "magic" in L.snc_b200_last_error().decode()
+    assert status(data[:len(data) // 2]) == _lib.EINVAL
+    assert "truncated" in L.snc_b200_last_error().decode()
+    assert status(data[:12]) == _lib.EINVAL
+    N, S = g.num_neurons, g.num_synapses
+    words = np.frombuffer(bytes(data), dtype="<i4").copy()
+    words[5 + 3 * S + 1] = 7  # a role outside 0..2
+    assert status(words.tobytes()) == _lib.EINVAL and "role" in L.snc_b200_last_error().decode()

@@ -103,3 +103,73 @@ def test_empty_graph():
     got, BS, P = _layout(dg, g)
     assert P == 1 and got["ibase"].tolist() == [0, 0] and got["gptr"].tolist() == [0]
     dg.release()
+
+
+# ---- SNCG files parsed and packed on the device --------------------------------
+
+def _sncg_bytes(g, tmp_path, with_weights=True):
+    from snc_b200.graph import save_sncg
+    p = tmp_path / "g.sncg"
+    save_sncg(g, p, with_weights=with_weights)
+    return p.read_bytes()
+
+
+@pytest.mark.parametrize("make", [lambda: W.random_graph(3, max_delay=9),
+                                  lambda: _many_blocks(1),
+                                  lambda: W.rec100k_graph(n=20000, width=200, seed=2)])
+@pytest.mark.parametrize("with_weights", [True, False])
+def test_sncg_device_ingest_equals_the_host_upload(make, with_weights, tmp_path):
+    """The delivery layout built from an SNCG file on the device equals the
+    layout of the same graph uploaded from host arrays (weights 1 and signs +1
+    when the file has no weights section), and the two uploads share the
+    autotuner's content hash."""
+    from snc_b200.graph import graph_from_sncg, load_graph
+    g = make()
+    data = _sncg_bytes(g, tmp_path, with_weights)
+    ref_g = graph_from_sncg(load_graph(tmp_path / "g.sncg"))
+    dg_file = R.DeviceGraph.from_sncg(data)
+    dg_host = R.DeviceGraph(ref_g)
+    a, bs_a, p_a = _layout(dg_file, ref_g)
+    b, bs_b, p_b = _layout(dg_host, ref_g)
+    assert (bs_a, p_a) == (bs_b, p_b)
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    assert (dg_file.N, dg_file.S, dg_file.n_in, dg_file.n_out) == (dg_host.N, dg_host.S, dg_host.n_in,
+                                                                   dg_host.n_out)
+    # the tuner keys both uploads alike: tuning one is found from the other
+    ev, steps = W.random_events(5, ref_g, 1, [20]) if ref_g.num_input_channels else \
+        (np.zeros(0, dtype=W.EVENT_DTYPE), [20])
+    di_h, di_f = R.DeviceInputs(dg_host, ev, steps), R.DeviceInputs(dg_file, ev, steps)
+    if ref_g.num_neurons <= 500:
+        R.autotune(dg_host, di_h, R.LIFParams())
+        assert R.autotune_lookup(dg_file, di_f) is not None
+
+
+def test_sncg_device_ingest_forward_and_rejections(tmp_path):
+    from oracle import oracle as O
+    g = W.random_graph(11, n_hid=80, max_delay=7)
+    data = bytearray(_sncg_bytes(g, tmp_path))
+    dg = R.DeviceGraph.from_sncg(bytes(data))
+    ev, steps = W.random_events(12, g, 2, [30, 25])
+    lif = R.LIFParams(refractory=1)
+    di = R.DeviceInputs(dg, ev, steps)
+    run = R.Run(dg, di, raster=True, vfinal=True)
+    run.launch(lif, mode=R.MODE_SORT, path=R.PATH_PERSISTENT)
+    out = run.fetch(raster=True, vfinal=True)
+    ref = O.forward_batched(g, ev, steps, lif)
+    for k in ("spikes", "events", "logits", "raster"):
+        assert np.array_equal(out[k], ref[k]), k
+    N, S = g.num_neurons, g.num_synapses
+    words = np.frombuffer(bytes(data), dtype="<i4").copy()
+    # offsets (in words) of pre, post, delays
+    o_pre, o_post, o_del = 5, 5 + S, 5 + 2 * S
+    cases = []
+    bad = words.copy(); bad[o_del + 3] = 0; cases.append((bad, _lib.EINVAL, "delay"))
+    bad = words.copy(); bad[o_del + 3] = 300; cases.append((bad, _lib.EUNSUPPORTED, "delay"))
+    bad = words.copy(); bad[o_post + 1] = N; cases.append((bad, _lib.EINVAL, "post"))
+    bad = words.copy(); bad[o_pre + 2], bad[o_pre + S - 1] = bad[o_pre + S - 1], bad[o_pre + 2]
+    cases.append((bad, _lib.EINVAL, "CSR order"))
+    for w, code, msg in cases:
+        with pytest.raises(_lib.SncB200Error) as ei:
+            R.DeviceGraph.from_sncg(w.tobytes())
+        assert ei.value.status == code and msg in str(ei.value), (msg, str(ei.value))
