@@ -358,6 +358,53 @@ def config_legs(reps=3):
     return out
 
 
+def graph_build_leg(g, host_build_s):
+    """Getting the 10M-synapse graph onto the device, three ways: the host
+    numpy build of rec100k (timed by the caller) followed by the upload of
+    its arrays (validation, hashing, device packing); the same graph's SNCG
+    file image parsed and packed on the device; and a graph of the same
+    shape (100k neurons on a 400 x 250 torus, 100 synapses each, delays 1-30)
+    generated on the device by the counter-based generator (its per-neuron
+    spec built on the host first).  Wall times of the calls."""
+    import torch
+    from snc_b200 import graph as G
+    from snc_b200 import runtime as R
+    from snc_b200 import workloads as W
+    out = {"host_numpy_build_s": host_build_s, "synapses": int(g.num_synapses)}
+    for name, fn in (("upload_host_arrays_ms", lambda: R.DeviceGraph(g)),):
+        t0 = time.perf_counter()
+        dg = fn()
+        torch.cuda.synchronize()
+        out[name] = 1e3 * (time.perf_counter() - t0)
+        dg.release()
+    with tempfile.NamedTemporaryFile(suffix=".sncg") as f:
+        G.save_sncg(g, f.name)
+        data = open(f.name, "rb").read()
+    ms = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        dg = R.DeviceGraph.from_sncg(data)
+        torch.cuda.synchronize()
+        ms.append(1e3 * (time.perf_counter() - t0))
+        dg.release()
+    out["sncg_device_ingest_ms"] = min(ms)
+    out["sncg_bytes"] = len(data)
+    t0 = time.perf_counter()
+    spec = W.grid_graph_spec(seed=1)
+    out["grid_spec_host_ms"] = 1e3 * (time.perf_counter() - t0)
+    ms = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        dg = R.DeviceGraph.generate_grid(spec)
+        torch.cuda.synchronize()
+        ms.append(1e3 * (time.perf_counter() - t0))
+        S = dg.S
+        dg.release()
+    out["device_generate_ms"] = min(ms)
+    out["device_generate_synapses"] = int(S)
+    return out
+
+
 REF_GPU_LIB = os.path.join(ROOT, "snc_b200", "adapter", "_build", "libsncref_gpu.so")
 REF_BACKENDS = {"atomic": 2, "bucket": 3, "sort": 4}  # the reference's Backend::Cuda* values
 
@@ -627,7 +674,9 @@ def our_arm(args):
     from snc_b200 import workloads as W
     R.set_device(local)
     lif = W.lif_tau20()
+    t_build = time.perf_counter()
     g = W.rec100k_graph(seed=1)
+    t_build = time.perf_counter() - t_build
     ev, steps = W.rec100k_inputs(g, 1, 1000, seed=1 + rank)
     dg = R.DeviceGraph(g)
     di = R.DeviceInputs(dg, ev, steps)
@@ -735,6 +784,7 @@ def our_arm(args):
                                      ref_counts if cpu["kind"] == "reference" else None)
         extra["configs"] = config_legs()
         extra["reference_gpu"] = reference_gpu_leg()
+        extra["graph_build"] = graph_build_leg(g, t_build)
         extra["bptt"] = bptt_leg()
 
     if rank == 0:

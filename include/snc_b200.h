@@ -156,6 +156,31 @@ int snc_b200_graph_release(snc_b200_graph* g);
  * copied to the device once and its edges are checked, counted and packed
  * there; the same validation and limits as snc_b200_graph_upload apply. */
 int snc_b200_graph_upload_sncg(const void* data, size_t bytes, snc_b200_graph** out);
+
+/* Generate a grid graph on the device (no reference counterpart: the
+ * reference builds every graph on the host; this is the benchmark's large
+ * recurrent substrate built where it runs).  N = width x height neurons on a
+ * torus (id = y * width + x), out_degree synapses per neuron: out_degree -
+ * long_range local targets at a displacement of standard deviation sigma
+ * per axis (an Irwin-Hall(4) variate), candidate j kept with probability
+ * accept[j] / 2^32 (the in-degree skew; from draw max_draws on every
+ * candidate is kept, 0 = 1000 x out_degree), then long_range targets uniform
+ * over all neurons; weights w_std x an Irwin-Hall(4) variate, delays uniform
+ * in 1..max_delay.  Every draw is a Philox-4x32-10 word keyed by seed and
+ * counted by (neuron, draw, stream) and every derived value is integer
+ * arithmetic or one correctly rounded float operation, so the graph is the
+ * same on any host (snc_b200.workloads.grid_graph_host builds it with
+ * numpy).  role, sign, channel [N] as in snc_graph_view. */
+typedef struct {
+  int32_t width, height;
+  int32_t out_degree, long_range;
+  float sigma, w_std;
+  int32_t max_delay; /* <= 255 */
+  int32_t max_draws;
+  uint64_t seed;
+} snc_grid_graph;
+int snc_b200_graph_generate_grid(const snc_grid_graph* p, const uint32_t* accept, const uint8_t* role,
+                                 const int8_t* sign, const int32_t* channel, snc_b200_graph** out);
 /* Basic shape: N, S, ring length, output channels, input channels. */
 int snc_b200_graph_info(const snc_b200_graph* g, int32_t* n, int32_t* s, int32_t* ring_len,
                         int32_t* n_out, int32_t* n_in);

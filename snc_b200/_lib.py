@@ -46,6 +46,12 @@ class LaunchConfig(C.Structure):
                 ("ms", C.c_float)]
 
 
+class GridGraph(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("out_degree", C.c_int32),
+                ("long_range", C.c_int32), ("sigma", C.c_float), ("w_std", C.c_float),
+                ("max_delay", C.c_int32), ("max_draws", C.c_int32), ("seed", C.c_uint64)]
+
+
 class RunStats(C.Structure):
     _fields_ = [("spikes", C.c_int64), ("synaptic_events", C.c_int64), ("overflow", C.c_int32),
                 ("ms", C.c_double)]
@@ -69,6 +75,7 @@ SIGNATURES = {
     "snc_b200_graph_upload": (C.c_int, [P, P]),
     "snc_b200_graph_release": (C.c_int, [P]),
     "snc_b200_graph_upload_sncg": (C.c_int, [P, C.c_size_t, P]),
+    "snc_b200_graph_generate_grid": (C.c_int, [P, P, P, P, P, P]),
     "snc_b200_graph_info": (C.c_int, [P, P, P, P, P, P]),
     "snc_b200_graph_layout": (C.c_int, [P] * 11),
     "snc_b200_inputs_upload": (C.c_int, [P, P, C.c_size_t, I32, P, P]),

@@ -192,6 +192,20 @@ __device__ __forceinline__ int lower_bound_i(const int* a, int lo, int hi, int x
   return lo;
 }
 
+// Philox-4x32 with 10 rounds (Salmon, Moraes, Dror, Shaw, "Parallel random
+// numbers: as easy as 1, 2, 3", SC 2011): counter c, key k.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const unsigned hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    const unsigned hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += 0x9E3779B9u;
+    k.y += 0xBB67AE85u;
+  }
+  return c;
+}
+
 // Edge packing: x = ring column (24 bits) | delay << 24, y = signed weight bits.
 __device__ __forceinline__ int edge_col(uint2 e) { return static_cast<int>(e.x & 0xFFFFFFu); }
 __device__ __forceinline__ int edge_delay(uint2 e) { return static_cast<int>(e.x >> 24); }

@@ -132,6 +132,22 @@ class DeviceGraph:
         check(lib().snc_b200_graph_upload_sncg(buf, len(data), C.byref(h)), "graph_upload_sncg")
         return cls(None, _handle=h)
 
+    @classmethod
+    def generate_grid(cls, spec: dict) -> "DeviceGraph":
+        """Generate a grid graph on the device (snc_b200_graph_generate_grid)
+        from a spec of snc_b200.workloads.grid_graph_spec."""
+        p = _lib.GridGraph(spec["width"], spec["height"], spec["out_degree"], spec["long_range"],
+                           spec["sigma"], spec["w_std"], spec["max_delay"], spec["max_draws"],
+                           spec["seed"])
+        acc = np.ascontiguousarray(spec["accept"], np.uint32)
+        role = np.ascontiguousarray(spec["role"], np.uint8)
+        sign = np.ascontiguousarray(spec["sign"], np.int8)
+        ch = np.ascontiguousarray(spec["channel"], np.int32)
+        h = C.c_void_p()
+        check(lib().snc_b200_graph_generate_grid(C.byref(p), ptr(acc), ptr(role), ptr(sign), ptr(ch),
+                                                 C.byref(h)), "graph_generate_grid")
+        return cls(None, _handle=h)
+
     def _info(self):
         n, s, r, no, ni = (C.c_int32() for _ in range(5))
         check(lib().snc_b200_graph_info(self.h, C.byref(n), C.byref(s), C.byref(r), C.byref(no),

@@ -328,3 +328,100 @@ def char_lm(seed=1, vocab=96, hidden=4096, fan_in=64, sigma=64.0, max_delay=8, B
     tokens = zipf_tokens(rng, vocab, B * (T + 1)).reshape(B, T + 1)
     return {"H": hidden, "vocab": vocab, "pre": pre, "post": post, "delays": d,
             "x": tokens[:, :T], "y": tokens[:, 1:]}
+
+
+# ---- grid graphs from a counter-based generator ---------------------------------
+# The rule snc_b200_graph_generate_grid runs on the device (csrc/generate.cu),
+# restated with numpy so the same graph can be built on a host: Philox-4x32-10
+# (Salmon et al., SC 2011) words counted by (neuron, draw, stream), integer
+# arithmetic and single correctly rounded float32 operations only.
+
+_PH_M0, _PH_M1 = np.uint64(0xD2511F53), np.uint64(0xCD9E8D57)
+_PH_W0, _PH_W1 = np.uint64(0x9E3779B9), np.uint64(0xBB67AE85)
+_U32 = np.uint64(0xFFFFFFFF)
+
+
+def _philox(c0, c1, c2, c3, seed):
+    """Philox-4x32-10 of counters (c0, c1, c2, c3) (uint32 arrays) under key
+    seed (64-bit); returns the four uint32 words."""
+    c = [np.asarray(x, np.uint64) & _U32 for x in (c0, c1, c2, c3)]
+    k0, k1 = np.uint64(seed & 0xFFFFFFFF), np.uint64((seed >> 32) & 0xFFFFFFFF)
+    for _ in range(10):
+        p0, p1 = _PH_M0 * c[0], _PH_M1 * c[2]
+        c = [((p1 >> np.uint64(32)) ^ c[1] ^ k0) & _U32, p1 & _U32,
+             ((p0 >> np.uint64(32)) ^ c[3] ^ k1) & _U32, p0 & _U32]
+        k0, k1 = (k0 + _PH_W0) & _U32, (k1 + _PH_W1) & _U32
+    return [x.astype(np.uint32) for x in c]
+
+
+def _halves_sum(a, b):
+    a, b = a.astype(np.int64), b.astype(np.int64)
+    return (a >> 16) + (a & 0xFFFF) + (b >> 16) + (b & 0xFFFF) - 131072
+
+
+def grid_graph_spec(seed=1, width=400, height=250, out_degree=100, long_range=5, sigma=4.0,
+                    w_std=0.05, max_delay=30, input_frac=0.1, n_out=10, max_draws=0) -> dict:
+    """Inputs of snc_b200_graph_generate_grid for a C2-style substrate (the
+    defaults: 100k neurons, 10M synapses, delays 1-30): per-neuron acceptance
+    thresholds from lognormal(0, 1) attractiveness capped at its 99.5 %
+    quantile (the heavy-tailed in-degree), 10 % INPUT neurons and n_out
+    OUTPUT neurons drawn with numpy from the seed."""
+    n = width * height
+    rng = np.random.default_rng([seed, 7])
+    attract = rng.lognormal(0.0, 1.0, n)
+    acc = np.minimum(attract / np.quantile(attract, 0.995), 1.0)
+    accept = np.minimum(np.floor(acc * 4294967296.0), 4294967295.0).astype(np.uint32)
+    role = np.full(n, INTERNAL, np.uint8)
+    channel = np.full(n, -1, np.int32)
+    inp = np.sort(rng.choice(n, int(n * input_frac), replace=False))
+    role[inp] = INPUT
+    channel[inp] = np.arange(inp.shape[0])
+    rest = np.setdiff1d(np.arange(n), inp)
+    outs = np.sort(rng.choice(rest, n_out, replace=False))
+    role[outs] = OUTPUT
+    channel[outs] = np.arange(n_out)
+    return {"width": width, "height": height, "out_degree": out_degree, "long_range": long_range,
+            "sigma": float(sigma), "w_std": float(w_std), "max_delay": max_delay,
+            "max_draws": max_draws, "seed": int(seed), "accept": accept, "role": role,
+            "sign": np.ones(n, np.int8), "channel": channel}
+
+
+def grid_graph_host(spec: dict) -> SNNGraph:
+    """The graph snc_b200_graph_generate_grid builds from `spec`, built on the
+    host (vectorised over neurons, one draw index at a time)."""
+    W, H, k, lr = spec["width"], spec["height"], spec["out_degree"], spec["long_range"]
+    n, k_loc, seed = W * H, k - lr, spec["seed"]
+    max_draws = spec["max_draws"] or 1000 * max(1, k)
+    c_disp = np.float32(spec["sigma"] * math.sqrt(3.0) / 65536.0)
+    c_w = np.float32(spec["w_std"] * math.sqrt(3.0) / 65536.0)
+    accept = np.asarray(spec["accept"], np.uint32)
+    posts = np.zeros((n, k), np.int32)
+    got = np.zeros(n, np.int64)
+    ids = np.arange(n)
+    x, y = ids % W, ids // W
+    d = 0
+    active = ids[got < k_loc]
+    while active.shape[0]:
+        r = _philox(active, np.full(active.shape, d), 0, 0, seed)
+        dx = np.rint(_halves_sum(r[0], r[1]).astype(np.float32) * c_disp).astype(np.int64)
+        dy = np.rint(_halves_sum(r[2], r[3]).astype(np.float32) * c_disp).astype(np.int64)
+        j = ((y[active] + dy) % H) * W + (x[active] + dx) % W
+        u = _philox(active, np.full(active.shape, d), 1, 0, seed)[0]
+        keep = (u < accept[j]) | (d >= max_draws)
+        a = active[keep]
+        posts[a, got[a]] = j[keep]
+        got[a] += 1
+        active = active[got[active] < k_loc]
+        d += 1
+    for q in range(lr):
+        u = _philox(ids, np.full(n, q), 2, 0, seed)[0]
+        posts[:, k_loc + q] = ((u.astype(np.uint64) * np.uint64(n)) >> np.uint64(32)).astype(np.int32)
+    w = np.zeros((n, k), np.float32)
+    dl = np.zeros((n, k), np.int32)
+    for s in range(k):
+        r = _philox(ids, np.full(n, s), 3, 0, seed)
+        w[:, s] = _halves_sum(r[0], r[1]).astype(np.float32) * c_w
+        dl[:, s] = 1 + ((r[2].astype(np.uint64) * np.uint64(spec["max_delay"])) >> np.uint64(32)).astype(np.int32)
+    row_ptr = (np.arange(n + 1, dtype=np.int64) * k).astype(np.int32)
+    return SNNGraph(n, row_ptr, posts.ravel(), w.ravel(), dl.ravel(), spec["role"], spec["sign"],
+                    spec["channel"])

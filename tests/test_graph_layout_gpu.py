@@ -173,3 +173,38 @@ def test_sncg_device_ingest_forward_and_rejections(tmp_path):
         with pytest.raises(_lib.SncB200Error) as ei:
             R.DeviceGraph.from_sncg(w.tobytes())
         assert ei.value.status == code and msg in str(ei.value), (msg, str(ei.value))
+
+
+# ---- grid graphs generated on the device ----------------------------------------
+
+@pytest.mark.parametrize("kw", [dict(seed=3, width=40, height=30, out_degree=24, long_range=3),
+                                dict(seed=9, width=64, height=50, out_degree=40, long_range=5,
+                                     sigma=6.0, max_delay=17),
+                                dict(seed=5, width=16, height=16, out_degree=8, long_range=0,
+                                     max_draws=3)])
+def test_device_grid_generator_equals_the_host_statement(kw):
+    """snc_b200_graph_generate_grid builds, bit for bit, the graph that
+    workloads.grid_graph_host builds from the same spec: the device layout
+    equals the statement's layout of the host graph (posts through the ring
+    columns, delays, weight bits, groups), and a SORT forward on it equals
+    the oracle on the host graph."""
+    from oracle import oracle as O
+    spec = W.grid_graph_spec(**kw)
+    g = W.grid_graph_host(spec)
+    assert g.validate() == ""
+    dg = R.DeviceGraph.generate_grid(spec)
+    assert (dg.N, dg.S) == (g.num_neurons, g.num_synapses)
+    got, BS, P = _layout(dg, g)
+    exp = _expected(g, BS)
+    assert P == exp["P"]
+    for k in ("edges", "gedges", "gptr", "groups", "col_of", "colbase", "ibase"):
+        assert np.array_equal(got[k], exp[k]), k
+    ev, steps = W.rec100k_inputs(g, 2, 60, rate=0.05, seed=kw["seed"])
+    lif = W.lif_tau20()
+    di = R.DeviceInputs(dg, ev, steps)
+    run = R.Run(dg, di, raster=True, vfinal=True)
+    run.launch(lif, mode=R.MODE_SORT, path=R.PATH_PERSISTENT)
+    out = run.fetch(raster=True, vfinal=True)
+    ref = O.forward_batched(g, ev, steps, lif)
+    for k in ("spikes", "events", "logits", "raster"):
+        assert np.array_equal(out[k], ref[k]), k
