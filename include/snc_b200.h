@@ -283,6 +283,35 @@ int snc_b200_forward_batched(const snc_b200_graph* graph, const snc_input_event*
                              const snc_lif* lif, int mode, float* logits, int64_t* spikes,
                              int64_t* events_out, snc_run_stats* stats);
 
+/* ---- post-neuron partitions ----------------------------------------------------
+ * One sample's forward split by post neuron across devices (the optional
+ * partitioned mode of a graph too large for one device; the reference runs
+ * one sample on one device, src/runtime/cuda_backend.cu:186-361).  A
+ * partition owns neuron blocks [block_lo, block_hi) of the graph's block
+ * partition (snc_b200_graph_layout's block_size / num_blocks): their state
+ * and delay-ring columns; every rank keeps the whole graph.  Per step t:
+ *   snc_b200_part_integrate  integrates the partition's neurons and writes
+ *       their spike bits into words [block_lo * BS / 32, block_hi * BS / 32)
+ *       of mask (DEVICE, ceil(N / 32) words; may be NULL);
+ *   the caller makes every partition's words available in every rank's
+ *       mask (an all-gather of the step's spike bits: 12.5 KB for 100k
+ *       neurons);
+ *   snc_b200_part_deliver  delivers every fired neuron's synapses into the
+ *       partition's columns in the serial CPU backend's (pre, edge) order.
+ * The ranks' results together equal one device's SORT run bit for bit.
+ * in holds one sample; lif as in snc_b200_run_launch.  fetch: logits (the
+ * partition's output spikes), spikes and events of the partition's neurons,
+ * the raster [T][ceil(N/32)] with the partition's bits, v_final [N] (valid
+ * for the partition's neurons).  Calls are ordered on `stream`. */
+typedef struct snc_b200_part snc_b200_part;
+int snc_b200_part_create(const snc_b200_graph* g, const snc_b200_inputs* in, int32_t block_lo,
+                         int32_t block_hi, const snc_lif* lif, snc_b200_part** out);
+int snc_b200_part_release(snc_b200_part* p);
+int snc_b200_part_integrate(snc_b200_part* p, int32_t t, uint32_t* mask, void* stream);
+int snc_b200_part_deliver(snc_b200_part* p, int32_t t, const uint32_t* mask, void* stream);
+int snc_b200_part_fetch(snc_b200_part* p, float* logits, int64_t* spikes, int64_t* events,
+                        uint32_t* raster, float* v_final);
+
 /* ---- launch shapes and the delivery autotuner ---------------------------------
  * No reference counterpart: the reference picks its backend by a flag
  * (src/bench/snc_bench.cpp:301-317).

@@ -92,6 +92,11 @@ SIGNATURES = {
     "snc_b200_autotune_ex": (C.c_int, [P, P, P, P, I32, P, P]),
     "snc_b200_autotune_lookup": (C.c_int, [P, P, P]),
     "snc_b200_run_configure": (C.c_int, [P, P]),
+    "snc_b200_part_create": (C.c_int, [P, P, I32, I32, P, P]),
+    "snc_b200_part_release": (C.c_int, [P]),
+    "snc_b200_part_integrate": (C.c_int, [P, I32, P, P]),
+    "snc_b200_part_deliver": (C.c_int, [P, I32, P, P]),
+    "snc_b200_part_fetch": (C.c_int, [P, P, P, P, P, P]),
     "snc_b200_run_set_readout": (C.c_int, [P, C.c_float]),
     "snc_b200_eprop_create": (C.c_int, [P, P, P, I32, P, P, P]),
     "snc_b200_eprop_release": (C.c_int, [P]),

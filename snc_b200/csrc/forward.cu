@@ -118,6 +118,12 @@ struct FwdArgs {
   int n_ro;
   float* ro_v;
   float* ro_logits;
+  // post-neuron partitions (plain kernels only): first neuron block of the
+  // grid, no inbox descriptors posted, delivery by scanning every block's
+  // fired list (SORT)
+  int blk0;
+  int no_post;
+  int scan_only;
 };
 
 // Shared-memory bytes of the tier-S kernel for this graph.
@@ -896,7 +902,7 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, unsigne
         }
       }
     }
-  } else {
+  } else if (!a.no_post) {
     // one descriptor (first edge, length) per destination block of each
     // fired row; a warp posts the groups of one row in parallel
     int* cnt = a.inbox_cnt + ((size_t)k * 2 + par) * P;
@@ -1098,6 +1104,10 @@ template <int MODE, bool RSM>
 __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, int t, int b,
                         int cb0, int cb1, bool tail_sync) {
   __shared__ int s_cnt;
+  if (MODE == MODE_SORT && a.scan_only) {  // partitions: no inbox, every fired list
+    phase_b_scan<RSM>(a, sm, scratch, k, t, b, cb0, cb1);
+    return;
+  }
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int R = a.R;
   const int par = t & 1;
@@ -1311,8 +1321,8 @@ __global__ void __launch_bounds__(kGThreads) k_plain_a(FwdArgs a, int sample, lo
   for (int jj = threadIdx.x; jj < a.BS; jj += blockDim.x) sm.ext[jj] = 0.f;
   for (int i = threadIdx.x; i <= a.P; i += blockDim.x) sm.ib[i] = a.ibase[i];
   __syncthreads();
-  phase_a<MODE, false, false>(a, sm, scratch, nullptr, 0, sample, gstep, t, blockIdx.x,
-                              a.colbase[blockIdx.x], false);
+  const int b = a.blk0 + blockIdx.x;
+  phase_a<MODE, false, false>(a, sm, scratch, nullptr, 0, sample, gstep, t, b, a.colbase[b], false);
 }
 
 template <int MODE>
@@ -1326,13 +1336,13 @@ __global__ void __launch_bounds__(kGThreads) k_plain_b(FwdArgs a, int t) {
   }
   for (int i = threadIdx.x; i <= a.P; i += blockDim.x) sm.ib[i] = a.ibase[i];
   __syncthreads();
-  phase_b<MODE, false>(a, sm, scratch, 0, t, blockIdx.x, a.colbase[blockIdx.x],
-                       a.colbase[blockIdx.x + 1], false);
+  const int b = a.blk0 + blockIdx.x;
+  phase_b<MODE, false>(a, sm, scratch, 0, t, b, a.colbase[b], a.colbase[b + 1], false);
 }
 
 // Zero wave slot 0's global state of block b (plain path, once per sample).
 __global__ void k_plain_init(FwdArgs a) {
-  const int b = blockIdx.x;
+  const int b = a.blk0 + blockIdx.x;
   const int lo = b * a.BS, hi = min(a.N, lo + a.BS);
   const int cb0 = a.colbase[b], cb1 = a.colbase[b + 1];
   for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
@@ -1760,4 +1770,189 @@ int launch_run(Run* r, const snc_lif* lif, int mode, int path, cudaStream_t st) 
   return SNC_B200_OK;
 }
 
+// ---------------------------------------------------------------------------
+// post-neuron partitions (one sample; the neuron-partitioned C2 mode)
+// ---------------------------------------------------------------------------
+// Rank r of a partitioned run owns neuron blocks [blk_lo, blk_hi) -- their
+// state and ring columns -- and keeps the whole graph.  Per step: integrate
+// the own blocks (k_plain_a without inbox posting; spike bits go to the
+// raster row of the step), exchange the raster row's words (the caller:
+// an all-gather), rebuild every block's ascending fired list from the full
+// row (k_mask_fired), then deliver into the own columns by scanning those
+// lists in (pre, edge) order (k_plain_b with scan_only): the contributions
+// of every ring cell arrive in the serial CPU backend's order, so the union
+// of the ranks' results equals a single-device run bit for bit.
+
+// Fired lists and counts of every block from one step's spike bits.
+__global__ void k_mask_fired(const uint32_t* __restrict__ mask, int N, int BS, int* fired,
+                             int* fired_cnt, int P) {
+  __shared__ int scratch[40];
+  const int b = blockIdx.x;
+  const int lo = b * BS, hi = min(N, lo + BS);
+  const int w0 = lo >> 5, w1 = (hi + 31) >> 5;  // BS is a multiple of 32
+  int base = 0;
+  for (int c0 = w0; c0 < w1; c0 += blockDim.x) {
+    const int w = c0 + threadIdx.x;
+    uint32_t m = w < w1 ? mask[w] : 0u;
+    if (w == w1 - 1 && (hi & 31)) m &= (1u << (hi & 31)) - 1u;  // bits beyond N
+    int tot;
+    const int ex = block_exclusive_scan(__popc(m), scratch, &tot);
+    int pos = base + ex;
+    while (m) {
+      const int bit = __ffs(m) - 1;
+      m &= m - 1u;
+      fired[lo + pos++] = (w << 5) + bit;
+    }
+    base += tot;
+  }
+  if (threadIdx.x == 0) fired_cnt[b] = base;
+}
+
+struct Part {
+  Run run;
+  int blk_lo = 0, blk_hi = 0;
+  snc_lif lif{};
+  FwdArgs a{};
+  size_t smem = 0;
+};
+
+static int part_create(const Graph* g, const Inputs* in, int blk_lo, int blk_hi, const snc_lif* lif,
+                       Part* p) {
+  if (in->B != 1) { set_error("partition: one sample per run"); return SNC_B200_EINVAL; }
+  if (blk_lo < 0 || blk_hi > g->P || blk_lo >= blk_hi) {
+    set_error("partition: blocks must satisfy 0 <= block_lo < block_hi <= num_blocks");
+    return SNC_B200_EINVAL;
+  }
+  Run* r = &p->run;
+  r->g = g;
+  r->in = in;
+  r->flags = SNC_B200_RUN_RASTER | SNC_B200_RUN_VFINAL;
+  r->W = (g->N + 31) / 32;
+  int rc;
+  if ((rc = dev_alloc(&r->counts, (size_t)std::max(1, g->noc)))) return rc;
+  if ((rc = dev_alloc(&r->spikes, 1))) return rc;
+  if ((rc = dev_alloc(&r->events, 1))) return rc;
+  if ((rc = dev_alloc(&r->raster, (size_t)std::max<long long>(1, in->raster_words)))) return rc;
+  if ((rc = dev_alloc(&r->vfinal, (size_t)std::max(1, g->N)))) return rc;
+  if ((rc = dev_alloc(&r->err, 1))) return rc;
+  if ((rc = dev_alloc(&r->ctl, 4))) return rc;
+  if ((rc = ensure_grid_state(r, 1))) return rc;
+  p->blk_lo = blk_lo;
+  p->blk_hi = blk_hi;
+  p->lif = *lif;
+  p->a = make_args(r, lif);
+  p->a.blk0 = blk_lo;
+  p->a.no_post = 1;
+  p->a.scan_only = 1;
+  p->smem = g_smem_bytes(g->BS, g->P, g->R, 1, false, false);
+  SNCB_CUDA(cudaFuncSetAttribute(k_plain_a<MODE_SORT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem));
+  SNCB_CUDA(cudaFuncSetAttribute(k_plain_b<MODE_SORT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem));
+  return SNC_B200_OK;
+}
+
+static int part_integrate(Part* p, int t, uint32_t* mask, cudaStream_t st) {
+  Run* r = &p->run;
+  const Graph* g = r->g;
+  const int T = r->in->steps_h[0];
+  if (t < 0 || t >= T) { set_error("partition: step outside the sample"); return SNC_B200_EINVAL; }
+  const int nb = p->blk_hi - p->blk_lo;
+  if (t == 0) {
+    SNCB_CUDA(cudaMemsetAsync(r->counts, 0, (size_t)std::max(1, g->noc) * sizeof(int), st));
+    SNCB_CUDA(cudaMemsetAsync(r->spikes, 0, sizeof(unsigned long long), st));
+    SNCB_CUDA(cudaMemsetAsync(r->events, 0, sizeof(unsigned long long), st));
+    SNCB_CUDA(cudaMemsetAsync(r->raster, 0, (size_t)std::max<long long>(1, r->in->raster_words) * 4, st));
+    k_plain_init<<<nb, kGThreads, 0, st>>>(p->a);
+  }
+  const long long gb = r->in->stepbase_h[0];
+  k_plain_a<MODE_SORT><<<nb, kGThreads, p->smem, st>>>(p->a, 0, gb + t, t);
+  SNCB_CUDA(cudaGetLastError());
+  if (mask) {  // this partition's words of the step's spike bits
+    const size_t w0 = (size_t)p->blk_lo * g->BS / 32;
+    const size_t w1 = std::min<size_t>((size_t)r->W, (size_t)p->blk_hi * g->BS / 32);
+    if (w1 > w0)
+      SNCB_CUDA(cudaMemcpyAsync(mask + w0, r->raster + (size_t)t * r->W + w0, (w1 - w0) * 4,
+                                cudaMemcpyDeviceToDevice, st));
+  }
+  return SNC_B200_OK;
+}
+
+static int part_deliver(Part* p, int t, const uint32_t* mask, cudaStream_t st) {
+  Run* r = &p->run;
+  const Graph* g = r->g;
+  const int par = t & 1;
+  k_mask_fired<<<g->P, 256, 0, st>>>(mask, g->N, g->BS, r->fired + (size_t)par * g->N,
+                                     r->fired_cnt + (size_t)par * g->P, g->P);
+  k_plain_b<MODE_SORT><<<p->blk_hi - p->blk_lo, kGThreads, p->smem, st>>>(p->a, t);
+  SNCB_CUDA(cudaGetLastError());
+  if (t == r->in->steps_h[0] - 1)
+    k_copy_v<<<std::max(1, std::min(1024, (g->N + 255) / 256)), 256, 0, st>>>(p->a, 0);
+  return SNC_B200_OK;
+}
+
 }  // namespace sncb
+
+struct snc_b200_part : sncb::Part {};
+
+using namespace sncb;
+
+extern "C" {
+
+int snc_b200_part_create(const snc_b200_graph* g, const snc_b200_inputs* in, int32_t block_lo,
+                         int32_t block_hi, const snc_lif* lif, snc_b200_part** out) {
+  if (!g || !in || !lif || !out) { set_error("null argument"); return SNC_B200_EINVAL; }
+  *out = nullptr;
+  auto* p = new snc_b200_part();
+  const int rc = part_create(g, in, block_lo, block_hi, lif, p);
+  if (rc) {
+    free_run(&p->run);
+    delete p;
+    return rc;
+  }
+  *out = p;
+  return SNC_B200_OK;
+}
+
+int snc_b200_part_release(snc_b200_part* p) {
+  if (!p) return SNC_B200_OK;
+  free_run(&p->run);
+  delete p;
+  return SNC_B200_OK;
+}
+
+int snc_b200_part_integrate(snc_b200_part* p, int32_t t, uint32_t* mask, void* stream) {
+  if (!p) { set_error("null partition"); return SNC_B200_EINVAL; }
+  return part_integrate(p, t, mask, static_cast<cudaStream_t>(stream));
+}
+
+int snc_b200_part_deliver(snc_b200_part* p, int32_t t, const uint32_t* mask, void* stream) {
+  if (!p || !mask) { set_error("null argument"); return SNC_B200_EINVAL; }
+  const int T = p->run.in->steps_h[0];
+  if (t < 0 || t >= T) { set_error("partition: step outside the sample"); return SNC_B200_EINVAL; }
+  return part_deliver(p, t, mask, static_cast<cudaStream_t>(stream));
+}
+
+int snc_b200_part_fetch(snc_b200_part* p, float* logits, int64_t* spikes, int64_t* events,
+                        uint32_t* raster, float* v_final) {
+  if (!p) { set_error("null partition"); return SNC_B200_EINVAL; }
+  SNCB_CUDA(cudaDeviceSynchronize());
+  int err = 0;
+  SNCB_CUDA(cudaMemcpy(&err, p->run.err, 4, cudaMemcpyDeviceToHost));
+  if (err) { set_error("device error word set"); return err < 0 ? err : SNC_B200_ECUDA; }
+  const Graph* g = p->run.g;
+  if (logits && g->noc) {
+    std::vector<int> c(g->noc);
+    SNCB_CUDA(cudaMemcpy(c.data(), p->run.counts, (size_t)g->noc * 4, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < g->noc; ++k) logits[k] = (float)c[k];
+  }
+  unsigned long long sp = 0, ev = 0;
+  SNCB_CUDA(cudaMemcpy(&sp, p->run.spikes, 8, cudaMemcpyDeviceToHost));
+  SNCB_CUDA(cudaMemcpy(&ev, p->run.events, 8, cudaMemcpyDeviceToHost));
+  if (spikes) *spikes = (int64_t)sp;
+  if (events) *events = (int64_t)ev;
+  if (raster && p->run.in->raster_words)
+    SNCB_CUDA(cudaMemcpy(raster, p->run.raster, (size_t)p->run.in->raster_words * 4, cudaMemcpyDeviceToHost));
+  if (v_final) SNCB_CUDA(cudaMemcpy(v_final, p->run.vfinal, (size_t)g->N * 4, cudaMemcpyDeviceToHost));
+  return SNC_B200_OK;
+}
+
+}  // extern "C"

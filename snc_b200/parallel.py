@@ -70,3 +70,117 @@ class DataParallelEprop:
             dist.all_reduce(grad, op=dist.ReduceOp.SUM, group=self.group)
         self.session.apply(grad, int(np.asarray(steps).shape[0]))
         return out
+
+
+def part_block_bounds(num_blocks: int, rank: int, world: int):
+    """Neuron blocks [lo, hi) of `rank` in a post-neuron partition: ceil(P /
+    world) blocks per rank, so rank r's spike-bit words start at r times one
+    rank's word count and an all-gather of equal chunks lands every word in
+    its place."""
+    per = -(-num_blocks // world)
+    lo = min(num_blocks, rank * per)
+    return lo, min(num_blocks, lo + per)
+
+
+class PartitionedForward:
+    """One sample's forward split by post neuron across ranks
+    (snc_b200_part_*): each rank owns a contiguous range of neuron blocks --
+    their state and ring columns -- and keeps the whole graph; per step the
+    ranks integrate their neurons, all-gather the step's spike bits (ceil(N /
+    32) words, 12.5 KB for 100k neurons: NCCL over NVLink on GPUs, landing in
+    local memory), and deliver every fired neuron's synapses into their own
+    columns in the CPU backend's order.  The ranks' results together equal a
+    single-device SORT run bit for bit.  world == 1 needs no process group."""
+
+    def __init__(self, dg, inputs, lif, rank=0, world=1, group=None):
+        import ctypes as C
+        import torch
+        from ._lib import check, lib
+        self.dg, self.inputs, self.rank, self.world, self.group = dg, inputs, rank, world, group
+        self.T = int(inputs.steps[0])
+        BS, P = dg.blocks()
+        self.BS, self.P = BS, P
+        self.blk = part_block_bounds(P, rank, world)
+        if self.blk[0] >= self.blk[1]:
+            raise ValueError("more ranks than neuron blocks")
+        self.chunk = -(-P // world) * BS // 32
+        self.words = (dg.N + 31) // 32
+        self.mask = torch.zeros(world * self.chunk, dtype=torch.int32, device="cuda")
+        lf = lif.c()
+        h = C.c_void_p()
+        check(lib().snc_b200_part_create(dg.h, inputs.h, self.blk[0], self.blk[1], C.byref(lf),
+                                         C.byref(h)), "part_create")
+        self.h = h
+
+    def run(self):
+        import ctypes as C
+        import torch
+        import torch.distributed as dist
+        from ._lib import check, lib
+        L = lib()
+        st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        mp = C.c_void_p(self.mask.data_ptr())
+        own = self.mask[self.rank * self.chunk:(self.rank + 1) * self.chunk]
+        for t in range(self.T):
+            check(L.snc_b200_part_integrate(self.h, t, mp, st), "part_integrate")
+            if self.world > 1:
+                dist.all_gather_into_tensor(self.mask, own.clone(), group=self.group)
+            check(L.snc_b200_part_deliver(self.h, t, mp, st), "part_deliver")
+        return self.fetch()
+
+    def fetch(self):
+        from ._lib import check, lib, ptr
+        N, noc = self.dg.N, max(1, self.dg.n_out)
+        logits = np.zeros(noc, np.float32)
+        sp, ev = np.zeros(1, np.int64), np.zeros(1, np.int64)
+        raster = np.zeros((self.T, self.words), np.uint32)
+        v = np.zeros(N, np.float32)
+        check(lib().snc_b200_part_fetch(self.h, ptr(logits), ptr(sp), ptr(ev), ptr(raster), ptr(v)),
+              "part_fetch")
+        lo, hi = self.blk[0] * self.BS, min(N, self.blk[1] * self.BS)
+        return {"logits": logits[:self.dg.n_out], "spikes": int(sp[0]), "events": int(ev[0]),
+                "raster": raster, "v": v[lo:hi], "neurons": (lo, hi)}
+
+    def release(self):
+        if getattr(self, "h", None):
+            from ._lib import lib
+            lib().snc_b200_part_release(self.h)
+            self.h = None
+
+
+def run_partitions_on_one_device(dg, inputs, lif, world):
+    """`world` partitions of one sample stepped in turn on the current device
+    with one shared spike-bit buffer (each step: every partition integrates,
+    then every partition delivers): the partitioned mode's kernels without a
+    process group.  Returns the per-partition results."""
+    import ctypes as C
+    import torch
+    from ._lib import check, lib
+    parts = [PartitionedForward.__new__(PartitionedForward) for _ in range(world)]
+    BS, P = dg.blocks()
+    chunk = -(-P // world) * BS // 32
+    mask = torch.zeros(world * chunk, dtype=torch.int32, device="cuda")
+    lf = lif.c()
+    for r, p in enumerate(parts):
+        p.dg, p.inputs, p.rank, p.world, p.group = dg, inputs, r, world, None
+        p.T, p.BS, p.P = int(inputs.steps[0]), BS, P
+        p.blk = part_block_bounds(P, r, world)
+        if p.blk[0] >= p.blk[1]:
+            raise ValueError("more partitions than neuron blocks")
+        p.chunk, p.words, p.mask = chunk, (dg.N + 31) // 32, mask
+        h = C.c_void_p()
+        check(lib().snc_b200_part_create(dg.h, inputs.h, p.blk[0], p.blk[1], C.byref(lf), C.byref(h)),
+              "part_create")
+        p.h = h
+    L = lib()
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    mp = C.c_void_p(mask.data_ptr())
+    for t in range(parts[0].T):
+        for p in parts:
+            check(L.snc_b200_part_integrate(p.h, t, mp, st), "part_integrate")
+        for p in parts:
+            check(L.snc_b200_part_deliver(p.h, t, mp, st), "part_deliver")
+    out = [p.fetch() for p in parts]
+    for p in parts:
+        p.release()
+    return out

@@ -148,6 +148,13 @@ class DeviceGraph:
                                                  C.byref(h)), "graph_generate_grid")
         return cls(None, _handle=h)
 
+    def blocks(self):
+        """(block_size, num_blocks) of the graph's neuron-block partition."""
+        bs, p = C.c_int32(), C.c_int32()
+        check(lib().snc_b200_graph_layout(self.h, *([None] * 7), C.byref(bs), C.byref(p), None),
+              "graph_layout")
+        return bs.value, p.value
+
     def _info(self):
         n, s, r, no, ni = (C.c_int32() for _ in range(5))
         check(lib().snc_b200_graph_info(self.h, C.byref(n), C.byref(s), C.byref(r), C.byref(no),

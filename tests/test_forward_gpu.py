@@ -358,3 +358,39 @@ def test_audio700_all_256_samples_leaky_readout(audio700_all):
     out = run.fetch(raster=True, vfinal=True)
     assert run.used_graph()
     assert_exact(out, ref)
+
+
+# ---- post-neuron partitions ------------------------------------------------------
+
+@pytest.mark.parametrize("world", [1, 2, 3])
+def test_partitions_on_one_device_equal_the_single_run(world):
+    """snc_b200_part_*: `world` partitions stepped in turn on one device with
+    a shared spike-bit buffer reproduce the single-device run bit for bit."""
+    from snc_b200 import parallel as PAR
+    g = W.rec100k_graph(seed=3, n=20000, width=200, out_degree=40, max_delay=20)
+    ev, steps = W.rec100k_inputs(g, 1, 300, rate=0.04, seed=3)
+    lif = W.lif_tau20()
+    ref = O.forward_batched(g, ev, steps, lif)
+    dg = R.DeviceGraph(g)
+    di = R.DeviceInputs(dg, ev, steps)
+    outs = PAR.run_partitions_on_one_device(dg, di, lif, world)
+    raster = np.bitwise_or.reduce([o["raster"] for o in outs])
+    np.testing.assert_array_equal(raster, ref["raster"])
+    v = np.concatenate([o["v"] for o in outs])
+    np.testing.assert_array_equal(v.view(np.uint32), ref["v"][0].view(np.uint32))
+    assert sum(o["spikes"] for o in outs) == int(ref["spikes"][0]) > 0
+    assert sum(o["events"] for o in outs) == int(ref["events"][0])
+    np.testing.assert_array_equal(np.sum([o["logits"] for o in outs], 0), ref["logits"][0])
+
+
+def test_partitions_on_the_bench_input(rec100k_bench):
+    """rec100k's benchmarked input (1000 steps) split over two partitions."""
+    from snc_b200 import parallel as PAR
+    g, ev, steps, lif, ref = rec100k_bench
+    dg = R.DeviceGraph(g)
+    di = R.DeviceInputs(dg, ev, steps)
+    outs = PAR.run_partitions_on_one_device(dg, di, lif, 2)
+    np.testing.assert_array_equal(np.bitwise_or.reduce([o["raster"] for o in outs]), ref["raster"])
+    v = np.concatenate([o["v"] for o in outs])
+    np.testing.assert_array_equal(v.view(np.uint32), ref["v"][0].view(np.uint32))
+    assert sum(o["events"] for o in outs) == int(ref["events"][0])

@@ -91,3 +91,66 @@ def test_data_parallel_eprop_gloo_world2(tmp_path):
                            lr=LR, w_max=WMAX, train_hidden=True, bmat=fb, labels=labels)
     assert np.abs(single["w"] - w0).max() > 0
     np.testing.assert_allclose(w_r0, single["w"], rtol=1e-5, atol=1e-6)
+
+
+# ---- post-neuron partitioned forward (restatement on gloo ranks) ---------------
+
+def part_case():
+    g = W.rec100k_graph(seed=4, n=3000, width=60, out_degree=30, long_range=3, max_delay=12)
+    ev, st = W.rec100k_inputs(g, 1, 120, rate=0.08, seed=2)
+    return g, ev, int(st[0]), W.lif_tau20()
+
+
+def _part_worker(rank, world, port, out):
+    from oracle import partition as OP
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        g, ev, T, lif = part_case()
+        N = g.num_neurons
+        bounds = [(r * N // world, (r + 1) * N // world) for r in range(world)]
+        lo, hi = bounds[rank]
+        width = max(h - l for l, h in bounds)
+
+        def gather(bits):
+            buf = torch.zeros(width, dtype=torch.uint8)
+            buf[:bits.shape[0]] = torch.from_numpy(bits.astype(np.uint8))
+            parts = [torch.zeros(width, dtype=torch.uint8) for _ in range(world)]
+            dist.all_gather(parts, buf)
+            return np.concatenate([p.numpy()[:h - l] for p, (l, h) in zip(parts, bounds)]).astype(bool)
+
+        r = OP.partition_forward(g, ev, T, lif, lo, hi, gather)
+        np.savez(os.path.join(out, f"part{rank}.npz"), raster=r["raster"], v=r["v"],
+                 counts=np.array([r["spikes"], r["events"]]), logits=r["logits"], lo=lo, hi=hi)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_partitioned_forward_gloo_world2_equals_single_rank(tmp_path):
+    """Two gloo ranks, each owning half of the neurons, exchange one step's
+    spike bits per step; together they reproduce the single-process forward
+    bit for bit (rasters, potentials, spike and event counts, logits)."""
+    port = 29700 + (os.getpid() % 1000)
+    mp.start_processes(_part_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    g, ev, T, lif = part_case()
+    ref = O.forward_batched(g, ev, np.array([T], np.int32), lif)
+    parts = [np.load(tmp_path / f"part{r}.npz") for r in range(2)]
+    raster = parts[0]["raster"] | parts[1]["raster"]
+    np.testing.assert_array_equal(raster, ref["raster"])
+    v = np.concatenate([p["v"] for p in parts])
+    np.testing.assert_array_equal(v.view(np.uint32), ref["v"][0].view(np.uint32))
+    assert sum(int(p["counts"][0]) for p in parts) == int(ref["spikes"][0]) > 0
+    assert sum(int(p["counts"][1]) for p in parts) == int(ref["events"][0])
+    np.testing.assert_array_equal(parts[0]["logits"] + parts[1]["logits"], ref["logits"][0])
+
+
+def test_part_block_bounds_cover_the_blocks():
+    for P in (1, 7, 125, 143):
+        for world in (1, 2, 3, 8):
+            if world > P:
+                continue
+            spans = [PAR.part_block_bounds(P, r, world) for r in range(world)]
+            assert spans[0][0] == 0 and spans[-1][1] == P
+            assert all(a[1] == b[0] for a, b in zip(spans, spans[1:]))
