@@ -761,6 +761,20 @@ def our_arm(args):
                            "mode": R.MODE_NAMES[m]}
             r2.release()
         extra["persistent_vs_plain_sort"] = extra["persistent_sort"]["events_per_s"] / extra["plain_sort"]["events_per_s"]
+        # the persistent loop's synchronisation floor: the same graph, launch
+        # shape, mode and 1000 steps with no drive (nothing fires: integration
+        # and the grid barrier of every step, no delivery)
+        di0 = R.DeviceInputs(dg, np.zeros(0, dtype=W.EVENT_DTYPE), steps)
+        r0 = R.Run(dg, di0, cuda_graph=True)
+        timed(r0, mode, R.PATH_PERSISTENT, 2)
+        ms0, _, sp0 = timed(r0, mode, R.PATH_PERSISTENT, k2)
+        r0.release()
+        di0.release()
+        floor_us = 1e3 * sum(ms0) / k2 / 1000
+        actual_us = 1e3 * ms_per_step / 1000
+        extra["sync_floor"] = {"us_per_step": floor_us, "actual_us_per_step": actual_us,
+                               "floor_over_actual": floor_us / actual_us, "spikes": int(sp0),
+                               "mode": R.MODE_NAMES[mode]}
 
     peak, peak_kind = peaks()
     per_launch_bytes = alg_bytes(ev_n / args.steps, sp_n / args.steps, g.num_neurons * 1000)
