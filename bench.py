@@ -57,7 +57,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--mode", default="auto", choices=["auto", "atomic", "bucket", "sort"])
     p.add_argument("--no-extra", action="store_true", help="skip the plain / sort / cpu legs")
-    p.add_argument("--leg", choices=["bptt", "bptt-custom", "configs", "reference-gpu"],
+    p.add_argument("--leg", choices=["bptt", "bptt-custom", "configs", "reference-gpu", "c3"],
                    help="run only this extra leg on one GPU and print its JSON (for profiling)")
     return p.parse_args()
 
@@ -237,6 +237,26 @@ def _time_cuda(fn, steps, warmup):
     t1.record()
     torch.cuda.synchronize()
     return t0.elapsed_time(t1) / steps
+
+
+def c3_leg(mode="sort", launches=3):
+    """C3 alone (audio700: 256 uneven samples, leaky readouts, persistent
+    path under a CUDA graph) in one delivery mode, `launches` launches: the
+    workload of the sample-per-CTA kernel's profiles."""
+    from snc_b200 import runtime as R
+    from snc_b200 import workloads as W
+    g = W.audio700_graph()
+    ev, steps = W.audio700_inputs(256)
+    dg = R.DeviceGraph(g)
+    di = R.DeviceInputs(dg, ev, steps)
+    run = R.Run(dg, di, cuda_graph=True)
+    run.set_readout(0.9)
+    m = {"atomic": R.MODE_ATOMIC, "sort": R.MODE_SORT}[mode]
+    ms = []
+    for _ in range(launches):
+        run.launch(W.lif_tau20(), mode=m, path=R.PATH_PERSISTENT)
+        ms.append(run.fetch()["ms"])
+    return {"mode": mode, "ms": ms}
 
 
 def config_legs(reps=3):
@@ -827,7 +847,8 @@ def main():
     args = parse()
     if args.leg:
         legs = {"bptt": bptt_leg, "bptt-custom": lambda: bptt_leg(with_reference=False),
-                "configs": config_legs, "reference-gpu": reference_gpu_leg}
+                "configs": config_legs, "reference-gpu": reference_gpu_leg,
+                "c3": lambda: c3_leg("atomic" if args.mode == "atomic" else "sort")}
         print(json.dumps({args.leg: legs[args.leg]()}), flush=True)
         return 0
     if args.impl == "reference":
