@@ -99,7 +99,7 @@ struct FwdArgs {
   float* elig;
   unsigned long long* fires;
   float gamma, trace_decay;
-  int s_table;  // tier S SORT: shared memory holds the whole-chunk cell table
+  int s_table;  // tier S SORT: 1 whole-chunk cell table, 2 large chunks with a packed table
   // deferred eligibility: psi of every ring column and step, [B][ncols][psi_T]
   // (null: eligibility accumulated in the forward into elig)
   float* psi_hist;
@@ -131,12 +131,21 @@ struct FwdArgs {
 // many list heads and one link per staged event.
 constexpr int kSTable = 2048;
 
+// Tier S SORT with large chunks (forward only): kBigChunk events per chunk,
+// a table of kBigTable packed entries (cell key << 13 | list head), a 16-bit
+// link and a weight per event -- in place of the four staging arrays.
+constexpr int kBigChunk = 4096;
+constexpr int kBigTable = 8192;
+constexpr int kBigKeyCols = (1 << 19) / 256 - 1;  // ring columns the 19-bit key holds
+
 static size_t tier_s_bytes(int N, int ncols, int R, int noc, int mode, bool eprop, int nthr,
-                           bool table = false) {
+                           int table = 0) {
   size_t words = (size_t)R * ncols + 4 * (size_t)N + (size_t)noc;
   if (mode == MODE_SORT) words += (size_t)N + 1 + 2 * (size_t)ncols + 4 * (size_t)nthr;
   if (eprop) words += (size_t)N + ncols;
-  if (mode == MODE_SORT && table) words += 2 * (size_t)kSTable + nthr;
+  if (mode == MODE_SORT && table == 1) words += 2 * (size_t)kSTable + nthr;
+  if (mode == MODE_SORT && table == 2)  // from st_col on: table, links, weights
+    words += kBigTable + kBigChunk / 2 + kBigChunk - 4 * (size_t)nthr;
   return words * 4 + 16;
 }
 
@@ -304,6 +313,80 @@ __device__ __forceinline__ void cell_apply(const int* tab, const int* link, cons
     }
     if (best == LLONG_MAX) break;
     apply_one<GLOBAL_RING>(ring, ring_stride, col0, c, sl, st_w[(int)(best & 1023)]);
+    last = best;
+  }
+}
+
+// Large-chunk variant of cell_insert / cell_apply (tier S SORT, s_table 2):
+// one 32-bit entry per cell holds its key (column * 256 + slot + 1, 19 bits)
+// and its list head (event + 1, 13 bits); links are 16-bit.  The thread that
+// claims an empty entry owns the cell.
+__device__ __forceinline__ unsigned big_insert(unsigned* tab, unsigned short* link, int q, int c, int sl,
+                                               bool* first) {
+  const unsigned key = (unsigned)c * 256u + (unsigned)sl + 1u;
+  const unsigned ent = (key << 13) | (unsigned)(q + 1);
+  unsigned h = (key * 2654435761u) >> (32 - 13);
+  // at most kBigChunk keys in kBigTable entries: a free or equal entry is found
+  for (int probe = 0; probe < (1 << 22); ++probe) {  // a failed CAS means another insert progressed
+    const unsigned old = *reinterpret_cast<volatile unsigned*>(&tab[h]);
+    const unsigned ok = old >> 13;
+    if (ok == 0u) {
+      if (atomicCAS(&tab[h], 0u, ent) == 0u) {
+        link[q] = 0;
+        *first = true;
+        return h;
+      }
+    } else if (ok == key) {
+      if (atomicCAS(&tab[h], old, ent) == old) {
+        link[q] = (unsigned short)(old & 8191u);
+        *first = false;
+        return h;
+      }
+    } else {
+      h = (h + 1u) & (kBigTable - 1);
+    }
+  }
+  *first = false;  // not reached: the table is never more than half full
+  return h;
+}
+
+__device__ __forceinline__ void big_apply(const unsigned* tab, const unsigned short* link, const float* w,
+                                          unsigned h, int q, int c, int sl, float* ring, int stride) {
+  const int top = (int)(tab[h] & 8191u);
+  if (top == q + 1) {
+    apply_one<false>(ring, stride, 0, c, sl, w[q]);
+    return;
+  }
+  int r[kCellSort];
+#pragma unroll
+  for (int i = 0; i < kCellSort; ++i) r[i] = INT_MAX;
+  int p = top;
+#pragma unroll
+  for (int i = 0; i < kCellSort; ++i) {
+    if (p != 0) {
+      r[kCellSort - 1] = p - 1;
+#pragma unroll
+      for (int m = kCellSort - 1; m > 0; --m) {
+        const int lo = min(r[m - 1], r[m]), hi = max(r[m - 1], r[m]);
+        r[m - 1] = lo;
+        r[m] = hi;
+      }
+      p = link[p - 1];
+    }
+  }
+  if (p == 0) {
+#pragma unroll
+    for (int i = 0; i < kCellSort; ++i)
+      if (r[i] != INT_MAX) apply_one<false>(ring, stride, 0, c, sl, w[r[i]]);
+    return;
+  }
+  int last = -1;
+  for (;;) {
+    int best = INT_MAX;
+    for (int x = top; x != 0; x = link[x - 1])
+      if (x - 1 > last && x - 1 < best) best = x - 1;
+    if (best == INT_MAX) break;
+    apply_one<false>(ring, stride, 0, c, sl, w[best]);
     last = best;
   }
 }
@@ -481,8 +564,14 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
   // SORT with a.s_table: the per-cell table for whole chunks (kSTable keys,
   // kSTable list heads, CH links)
   int* ctab = reinterpret_cast<int*>(EP ? psi + nc : tr);
-  if (MODE == MODE_SORT && a.s_table)
+  if (MODE == MODE_SORT && a.s_table == 1)
     for (int i = tid; i < 2 * kSTable; i += nthr) ctab[i] = 0;  // ordered by the loop's first barrier
+  // s_table 2: the packed table, links and weights from st_col on
+  unsigned* btab = reinterpret_cast<unsigned*>(st_col);
+  unsigned short* blink = reinterpret_cast<unsigned short*>(btab + kBigTable);
+  float* bw = reinterpret_cast<float*>(blink + kBigChunk);
+  if (MODE == MODE_SORT && !EP && a.s_table == 2)
+    for (int i = tid; i < kBigTable; i += nthr) btab[i] = 0u;
 
   for (;;) {
     if (tid == 0) s_q = (int)atomicAdd(&a.ctl[1], 1u);
@@ -611,7 +700,53 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
         }
         __syncthreads();
         const int E = base;
-        if (a.s_table) {
+        if (!EP && a.s_table == 2) {
+          // large chunks: each thread stages events tid + k * nthr of a
+          // kBigChunk chunk (their loads issued together), enters them in
+          // their cells' lists, and after one barrier the cell owners apply
+          // and clear -- two barriers per 4096 events
+          constexpr int kPer = kBigChunk / 1024;
+          auto edge_of = [&](int e) {
+            const int k = upper_index(pref, nf, e);
+            return a.edges[fired[k] + (e - pref[k])];
+          };
+          for (int e0 = 0; e0 < E; e0 += kBigChunk) {
+            const int ce = min(kBigChunk, E - e0);
+            uint2 ed[kPer];
+#pragma unroll
+            for (int k = 0; k < kPer; ++k) {
+              const int qq = tid + k * nthr;
+              ed[k] = qq < ce ? edge_of(e0 + qq) : make_uint2(0u, 0u);
+            }
+            unsigned hq[kPer];
+            int cq[kPer], sq[kPer];
+            bool own[kPer];
+#pragma unroll
+            for (int k = 0; k < kPer; ++k) {
+              const int qq = tid + k * nthr;
+              own[k] = false;
+              hq[k] = 0u;
+              cq[k] = sq[k] = 0;
+              if (qq < ce) {
+                sq[k] = ring_slot(s0, edge_delay(ed[k]), R);
+                cq[k] = edge_col(ed[k]);
+                bw[qq] = edge_w(ed[k]);
+                hq[k] = big_insert(btab, blink, qq, cq[k], sq[k], &own[k]);
+              }
+            }
+            __syncthreads();
+            // each owner clears its own entry once it has applied the cell
+            // (nobody else reads it before the next chunk), so the table is
+            // all zero again at the barrier
+#pragma unroll
+            for (int k = 0; k < kPer; ++k)
+              if (own[k]) {
+                big_apply(btab, blink, bw, hq[k], tid + k * nthr, cq[k], sq[k], ring, nc);
+                btab[hq[k]] = 0u;
+              }
+            __syncthreads();
+          }
+        } else if (a.s_table) {
           // per-cell apply of whole chunks (CH = blockDim.x: thread q stages
           // event q of the chunk and enters it in its cell's list; staging
           // order is the (pre, edge) order)
@@ -1442,9 +1577,26 @@ static int launch_tier_s_kernel(const Graph* g, int B, const FwdArgs& a_in, cuda
   int per_sm = 0;
   SNCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tier_s<MODE, EP>, nthr, smem));
   a.s_table = 0;
-  if (MODE == MODE_SORT) {
+  if (MODE == MODE_SORT && !EP && g->ncols <= kBigKeyCols) {
+    // large chunks when they fit without costing a CTA per SM
+    const size_t smem_b = tier_s_bytes(g->N, g->ncols, g->R, a.noc, MODE, EP, nthr, 2);
+    int per_sm_b = 0;
+    if ((int)smem_b <= optin_smem() &&
+        cudaFuncSetAttribute(k_tier_s<MODE, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b) ==
+            cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_b, k_tier_s<MODE, EP>, nthr, smem_b) ==
+            cudaSuccess &&
+        per_sm_b >= per_sm && per_sm_b >= 1) {
+      smem = smem_b;
+      a.s_table = 2;
+    } else {
+      cudaGetLastError();
+      SNCB_CUDA(cudaFuncSetAttribute(k_tier_s<MODE, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+  }
+  if (MODE == MODE_SORT && a.s_table == 0) {
     // the per-cell table when it fits without costing a CTA per SM
-    const size_t smem_t = tier_s_bytes(g->N, g->ncols, g->R, a.noc, MODE, EP, nthr, true);
+    const size_t smem_t = tier_s_bytes(g->N, g->ncols, g->R, a.noc, MODE, EP, nthr, 1);
     int per_sm_t = 0;
     if ((int)smem_t <= optin_smem() &&
         cudaFuncSetAttribute(k_tier_s<MODE, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t) ==
