@@ -471,7 +471,7 @@ class RefGpu:
         return {"ms": ms, "wall_ms": wall.value, "spikes": sp.value, "events": en.value}
 
 
-def reference_gpu_leg(budget_s=40.0):
+def reference_gpu_leg(budget_s=40.0, g_c2=None):
     """The reference's GPU kernels beside this backend's on the same B200 and
     the same inputs, in the reference's LIF semantics (reset to 0: it has no
     subtractive reset), forward of every delivery mode:
@@ -501,11 +501,13 @@ def reference_gpu_leg(budget_s=40.0):
                       refractory=lif0.refractory, reset_mode=0)
     out = {"lif": "threshold 1, decay exp(-1/20), reset to 0, refractory 0 (the reference's semantics)"}
     t_start = time.perf_counter()
-    for name, g, (ev, steps) in (("C1_ff784", W.ff784_graph(), W.ff784_inputs(64)),
-                                 ("C2_rec100k", W.rec100k_graph(seed=1), None),
-                                 ("C3_audio700_32", W.audio700_graph(), W.audio700_inputs(256))):
-        if name == "C2_rec100k":
-            ev, steps = W.rec100k_inputs(g, 1, 1000, seed=1)
+    for name, make_g, make_in in (
+            ("C1_ff784", W.ff784_graph, lambda g: W.ff784_inputs(64)),
+            ("C2_rec100k", lambda: g_c2 if g_c2 is not None else W.rec100k_graph(seed=1),
+             lambda g: W.rec100k_inputs(g, 1, 1000, seed=1)),
+            ("C3_audio700_32", W.audio700_graph, lambda g: W.audio700_inputs(256))):
+        g = make_g()
+        ev, steps = make_in(g)
         if name.startswith("C3"):
             keep = np.arange(32)
             ev = ev[np.isin(ev["sample_id"], keep)]
@@ -817,7 +819,7 @@ def our_arm(args):
         extra["parity"] = parity_leg(dg, di, g, ev, lif, mode, timed_out,
                                      ref_counts if cpu["kind"] == "reference" else None)
         extra["configs"] = config_legs()
-        extra["reference_gpu"] = reference_gpu_leg()
+        extra["reference_gpu"] = reference_gpu_leg(g_c2=g)
         extra["graph_build"] = graph_build_leg(g, t_build)
         extra["bptt"] = bptt_leg()
 

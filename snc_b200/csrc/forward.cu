@@ -2009,6 +2009,8 @@ static int part_integrate(Part* p, int t, uint32_t* mask, cudaStream_t st) {
   if (t < 0 || t >= T) { set_error("partition: step outside the sample"); return SNC_B200_EINVAL; }
   const int nb = p->blk_hi - p->blk_lo;
   if (t == 0) {
+    SNCB_CUDA(cudaMemsetAsync(r->err, 0, sizeof(int), st));
+    SNCB_CUDA(cudaMemsetAsync(r->ctl, 0, 4 * sizeof(unsigned), st));
     SNCB_CUDA(cudaMemsetAsync(r->counts, 0, (size_t)std::max(1, g->noc) * sizeof(int), st));
     SNCB_CUDA(cudaMemsetAsync(r->spikes, 0, sizeof(unsigned long long), st));
     SNCB_CUDA(cudaMemsetAsync(r->events, 0, sizeof(unsigned long long), st));
