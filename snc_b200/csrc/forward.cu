@@ -231,13 +231,11 @@ constexpr int kFirstFlag = 1 << 30;  // marks a group's first event of its colum
 // keys (column, slot) -- zeroed by the caller before staging -- holds one
 // unordered list per cell (atomicExch heads, one link per event).  The first
 // arrival at a cell owns it: alone there, it applies its event; otherwise it
-// collects the cell's list (kCellSort entries in registers, sorted; longer
-// lists by repeated minimum selection) and applies it in order.  A step's
+// applies the cell's list in order by repeated minimum selection.  A step's
 // events spread over many more cells than columns -- a column's events carry
 // different delays -- so lists are short and no thread walks a hub column's
 // whole chain.
 constexpr int kCellTable = 2 * kCountMax;  // keys, then list heads (q + 1, 0 = empty)
-constexpr int kCellSort = 8;
 static_assert(2 * kCellTable <= kGChunk, "the table lives in st_next");
 static_assert(kCellTable + kCountMax <= kGChunk, "the links live in st_col beyond the chunk");
 
@@ -280,30 +278,8 @@ __device__ __forceinline__ void cell_apply(const int* tab, const int* link, cons
   auto ord = [&](int x) -> long long {
     return KEYED ? ((long long)okey[x] << 10) | x : (long long)x;  // x < kGChunk = 1024
   };
-  long long r[kCellSort];
-#pragma unroll
-  for (int i = 0; i < kCellSort; ++i) r[i] = LLONG_MAX;
-  int p = top;
-#pragma unroll
-  for (int i = 0; i < kCellSort; ++i) {
-    if (p != 0) {
-      // insert into the sorted r (its largest entry is free)
-      r[kCellSort - 1] = ord(p - 1);
-#pragma unroll
-      for (int m = kCellSort - 1; m > 0; --m) {
-        const long long lo = min(r[m - 1], r[m]), hi = max(r[m - 1], r[m]);
-        r[m - 1] = lo;
-        r[m] = hi;
-      }
-      p = link[p - 1];
-    }
-  }
-  if (p == 0) {
-#pragma unroll
-    for (int i = 0; i < kCellSort; ++i)
-      if (r[i] != LLONG_MAX) apply_one<GLOBAL_RING>(ring, ring_stride, col0, c, sl, st_w[(int)(r[i] & 1023)]);
-    return;
-  }
+  // lists are short (a step's events spread over many cells): repeated
+  // minimum selection
   long long last = -1;
   for (;;) {
     long long best = LLONG_MAX;
@@ -317,70 +293,41 @@ __device__ __forceinline__ void cell_apply(const int* tab, const int* link, cons
   }
 }
 
-// Large-chunk variant of cell_insert / cell_apply (tier S SORT, s_table 2):
-// one 32-bit entry per cell holds its key (column * 256 + slot + 1, 19 bits)
-// and its list head (event + 1, 13 bits); links are 16-bit.  The thread that
-// claims an empty entry owns the cell.
-__device__ __forceinline__ unsigned big_insert(unsigned* tab, unsigned short* link, int q, int c, int sl,
-                                               bool* first) {
+// Large-chunk cell table (tier S SORT, s_table 2): one 32-bit entry per
+// cell holds its key (column * 256 + slot + 1, 19 bits) and its list head
+// (event + 1, 13 bits); links are 16-bit.
+__device__ __forceinline__ void big_insert(unsigned* tab, unsigned short* link, int q, int c, int sl) {
   const unsigned key = (unsigned)c * 256u + (unsigned)sl + 1u;
   const unsigned ent = (key << 13) | (unsigned)(q + 1);
   unsigned h = (key * 2654435761u) >> (32 - 13);
-  // at most kBigChunk keys in kBigTable entries: a free or equal entry is found
-  for (int probe = 0; probe < (1 << 22); ++probe) {  // a failed CAS means another insert progressed
+  // at most kBigChunk keys in kBigTable entries: a free or equal entry is
+  // always found; a failed CAS means another insert made progress
+  for (int probe = 0; probe < (1 << 22); ++probe) {
     const unsigned old = *reinterpret_cast<volatile unsigned*>(&tab[h]);
     const unsigned ok = old >> 13;
-    if (ok == 0u) {
-      if (atomicCAS(&tab[h], 0u, ent) == 0u) {
-        link[q] = 0;
-        *first = true;
-        return h;
-      }
-    } else if (ok == key) {
+    if (ok == 0u || ok == key) {
       if (atomicCAS(&tab[h], old, ent) == old) {
-        link[q] = (unsigned short)(old & 8191u);
-        *first = false;
-        return h;
+        link[q] = (unsigned short)(old & 8191u);  // 0: the cell's first event
+        return;
       }
     } else {
       h = (h + 1u) & (kBigTable - 1);
     }
   }
-  *first = false;  // not reached: the table is never more than half full
-  return h;
 }
 
-__device__ __forceinline__ void big_apply(const unsigned* tab, const unsigned short* link, const float* w,
-                                          unsigned h, int q, int c, int sl, float* ring, int stride) {
-  const int top = (int)(tab[h] & 8191u);
-  if (top == q + 1) {
-    apply_one<false>(ring, stride, 0, c, sl, w[q]);
+// Applies the events of one table entry (after the barrier that follows the
+// inserts) to its ring cell in increasing staging index.
+__device__ __forceinline__ void big_apply(unsigned ent, const unsigned short* link, const float* w,
+                                          float* ring, int stride) {
+  const unsigned key = (ent >> 13) - 1u;
+  const int c = (int)(key >> 8), sl = (int)(key & 255u);
+  const int top = (int)(ent & 8191u);
+  if (link[top - 1] == 0) {  // one event
+    apply_one<false>(ring, stride, 0, c, sl, w[top - 1]);
     return;
   }
-  int r[kCellSort];
-#pragma unroll
-  for (int i = 0; i < kCellSort; ++i) r[i] = INT_MAX;
-  int p = top;
-#pragma unroll
-  for (int i = 0; i < kCellSort; ++i) {
-    if (p != 0) {
-      r[kCellSort - 1] = p - 1;
-#pragma unroll
-      for (int m = kCellSort - 1; m > 0; --m) {
-        const int lo = min(r[m - 1], r[m]), hi = max(r[m - 1], r[m]);
-        r[m - 1] = lo;
-        r[m] = hi;
-      }
-      p = link[p - 1];
-    }
-  }
-  if (p == 0) {
-#pragma unroll
-    for (int i = 0; i < kCellSort; ++i)
-      if (r[i] != INT_MAX) apply_one<false>(ring, stride, 0, c, sl, w[r[i]]);
-    return;
-  }
-  int last = -1;
+  int last = -1;  // short lists: repeated minimum selection
   for (;;) {
     int best = INT_MAX;
     for (int x = top; x != 0; x = link[x - 1])
@@ -701,49 +648,32 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
         __syncthreads();
         const int E = base;
         if (!EP && a.s_table == 2) {
-          // large chunks: each thread stages events tid + k * nthr of a
-          // kBigChunk chunk (their loads issued together), enters them in
-          // their cells' lists, and after one barrier the cell owners apply
-          // and clear -- two barriers per 4096 events
-          constexpr int kPer = kBigChunk / 1024;
-          auto edge_of = [&](int e) {
-            const int k = upper_index(pref, nf, e);
-            return a.edges[fired[k] + (e - pref[k])];
-          };
+          // large chunks (kBigChunk events; staging position q = event index
+          // - e0 is the (pre, edge) order): a warp per fired row enters the
+          // row's events of the chunk in their cells' lists -- no search for
+          // an event's row -- and after one barrier every thread walks its
+          // share of the table, applying each cell's list in increasing q
+          // and clearing the entry: two barriers per 4096 events
           for (int e0 = 0; e0 < E; e0 += kBigChunk) {
-            const int ce = min(kBigChunk, E - e0);
-            uint2 ed[kPer];
-#pragma unroll
-            for (int k = 0; k < kPer; ++k) {
-              const int qq = tid + k * nthr;
-              ed[k] = qq < ce ? edge_of(e0 + qq) : make_uint2(0u, 0u);
-            }
-            unsigned hq[kPer];
-            int cq[kPer], sq[kPer];
-            bool own[kPer];
-#pragma unroll
-            for (int k = 0; k < kPer; ++k) {
-              const int qq = tid + k * nthr;
-              own[k] = false;
-              hq[k] = 0u;
-              cq[k] = sq[k] = 0;
-              if (qq < ce) {
-                sq[k] = ring_slot(s0, edge_delay(ed[k]), R);
-                cq[k] = edge_col(ed[k]);
-                bw[qq] = edge_w(ed[k]);
-                hq[k] = big_insert(btab, blink, qq, cq[k], sq[k], &own[k]);
+            const int e1 = min(E, e0 + kBigChunk);
+            for (int k = warp; k < nf; k += nwarps) {
+              const int p0 = pref[k], p1 = k + 1 < nf ? pref[k + 1] : E;
+              if (p1 <= e0 || p0 >= e1) continue;  // warp-uniform
+              const int rs = fired[k] - p0;  // edge of event e: rs + e
+              for (int e = max(p0, e0) + lane; e < min(p1, e1); e += 32) {
+                const uint2 ed = a.edges[rs + e];
+                const int q = e - e0;
+                bw[q] = edge_w(ed);
+                big_insert(btab, blink, q, edge_col(ed), ring_slot(s0, edge_delay(ed), R));
               }
             }
             __syncthreads();
-            // each owner clears its own entry once it has applied the cell
-            // (nobody else reads it before the next chunk), so the table is
-            // all zero again at the barrier
-#pragma unroll
-            for (int k = 0; k < kPer; ++k)
-              if (own[k]) {
-                big_apply(btab, blink, bw, hq[k], tid + k * nthr, cq[k], sq[k], ring, nc);
-                btab[hq[k]] = 0u;
-              }
+            for (int h = tid; h < kBigTable; h += nthr) {
+              const unsigned ent = btab[h];
+              if (ent == 0u) continue;
+              big_apply(ent, blink, bw, ring, nc);
+              btab[h] = 0u;
+            }
             __syncthreads();
           }
         } else if (a.s_table) {
