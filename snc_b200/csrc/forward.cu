@@ -1159,6 +1159,107 @@ __device__ bool phase_b_fast(const FwdArgs& a, const GSmem& sm, int k, int t, in
   return true;
 }
 
+// Phase B for a step whose descriptors warp 0 read while it waited on the
+// grid barrier (grid_wait_box; lane l holds slots l and l + 32, zero where it
+// saw none).  Slots are zero until posted and zeroed again once consumed, so
+// the leading run of non-zero slots is a prefix of this step's descriptors:
+// its events' edges are requested at once, while thread 0 reads the count in
+// the same round trip.  When the count equals the prefix (the common case)
+// the step is applied as in phase_b_fast; otherwise -- a post the wait did
+// not see, or more events than one per thread -- nothing has been applied
+// and false sends the step to the regular path.
+template <int MODE, bool RSM>
+__device__ bool phase_b_spec(const FwdArgs& a, const GSmem& sm, int k, int t, int b, int cb0,
+                             unsigned long long d0, unsigned long long d1, bool tail_sync) {
+  __shared__ int s_E, s_cs, s_cnt;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int par = t & 1;
+  int* cntp = a.inbox_cnt + ((size_t)k * 2 + par) * a.P + b;
+  unsigned long long* box = a.inbox + ((size_t)k * 2 + par) * a.G + sm.ib[b];
+  int* tab = reinterpret_cast<int*>(sm.desc);
+  constexpr int kMax = kFastDesc;
+  int cnt_reg = 0;
+  if (tid == 0) cnt_reg = __ldcg(cntp);  // used after the next barrier
+  if (tid < 32) {
+    const unsigned m0 = __ballot_sync(0xffffffffu, d0 != 0ull), m1 = __ballot_sync(0xffffffffu, d1 != 0ull);
+    int cs = m0 != 0xffffffffu ? __ffs(~m0) - 1 : 32 + (m1 != 0xffffffffu ? __ffs(~m1) - 1 : 32);
+    cs = min(cs, kMax);
+    const int l0 = tid < cs ? (int)(d0 & 0xffffffffu) : 0;
+    const int l1 = tid + 32 < cs ? (int)(d1 & 0xffffffffu) : 0;
+    int i0 = l0, i1 = l1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y0 = __shfl_up_sync(0xffffffffu, i0, o), y1 = __shfl_up_sync(0xffffffffu, i1, o);
+      if (tid >= o) {
+        i0 += y0;
+        i1 += y1;
+      }
+    }
+    const int t0 = __shfl_sync(0xffffffffu, i0, 31);
+    if (tid < cs) {
+      sm.dsort[tid] = d0;
+      sm.seg_p[tid] = i0 - l0;
+    }
+    if (tid + 32 < cs) {
+      sm.dsort[tid + 32] = d1;
+      sm.seg_p[tid + 32] = t0 + i1 - l1;
+    }
+    if (tid == 31) {
+      s_E = t0 + i1;
+      s_cs = cs;
+    }
+  }
+  if (MODE == MODE_SORT)
+    for (int i = tid; i < 2 * 2 * kFastMax; i += nthr) tab[i] = 0;
+  __syncthreads();
+  const int E = s_E, cs = s_cs;
+  const bool fits = E <= nthr && (MODE != MODE_SORT || E <= kFastMax);  // block-uniform
+  const int q = tid;
+  int edge = 0;
+  uint2 ed = make_uint2(0u, 0u);
+  if (fits && q < E) {
+    const int d = upper_index(sm.seg_p, cs, q);
+    edge = (int)(sm.dsort[d] >> 32) + (q - sm.seg_p[d]);
+    ed = a.gedges[edge];
+  }
+  if (tid == 0) s_cnt = cnt_reg;
+  __syncthreads();
+  const int cnt = s_cnt;
+  if (!fits || cnt != cs) return false;
+  if (cnt == 0) return true;
+  // consumed: the slots and the count are cleared for step t + 2
+  if (tid < cnt) __stcg(&box[tid], 0ull);
+  if (tid == 0) __stcg(cntp, 0);
+  const int R = a.R, s0 = t % R;
+  float* rb = ring_base<RSM>(a, sm, k);
+  const int stride = RSM ? a.BS : a.ncols;
+  const int col0 = RSM ? 0 : cb0;
+  if (MODE == MODE_BUCKET) {
+    if (q < E) {
+      const int cidx = RSM ? edge_col(ed) - cb0 : edge_col(ed);
+      atomicAdd(&rb[(size_t)ring_slot(s0, edge_delay(ed), R) * stride + cidx], edge_w(ed));
+    }
+    if (tail_sync) __syncthreads();
+    return true;
+  }
+  int c = 0, sl = 0;
+  unsigned h = 0;
+  bool first = false;
+  if (q < E) {
+    sl = ring_slot(s0, edge_delay(ed), R);
+    c = edge_col(ed) - cb0;
+    sm.st_w[q] = edge_w(ed);
+    sm.st_slot[q] = edge;  // order key
+    h = cell_insert<2 * kFastMax>(tab, sm.st_col, q, c, sl, &first);
+  }
+  __syncthreads();
+  if (first)
+    cell_apply<!RSM, true, 2 * kFastMax>(tab, sm.st_col, sm.st_slot, sm.st_w, h, q, c, sl, rb, stride,
+                                         col0);
+  if (tail_sync) __syncthreads();
+  return true;
+}
+
 // Phase B (BUCKET / SORT): as owner of the ring columns of block b, expand
 // this step's inbox descriptors and accumulate them into the block's ring
 // slice -- unordered (BUCKET) or per ring cell in (pre, edge) order (SORT).
@@ -1178,9 +1279,9 @@ __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, 
   const int par = t & 1;
   const int s0 = t % R;
   int* cntp = a.inbox_cnt + ((size_t)k * 2 + par) * a.P + b;
-  const unsigned long long* box = a.inbox + ((size_t)k * 2 + par) * a.G + sm.ib[b];
+  unsigned long long* box = a.inbox + ((size_t)k * 2 + par) * a.G + sm.ib[b];
   // read the first descriptor slots in the same round trip as the count
-  // (slots beyond the count hold stale descriptors and are ignored)
+  // (slots beyond the count are zero)
   const int cap = sm.ib[b + 1] - sm.ib[b];
   unsigned long long spec = 0, spec2 = 0;
   if (tid < kGDesc && tid < cap) spec = __ldcg(&box[tid]);
@@ -1193,10 +1294,20 @@ __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, 
   __syncthreads();
   const int cnt = s_cnt;
   if (cnt == 0) return;
+  // the slots this step filled are zeroed once read (by then every read of
+  // them is done), so that before the next posts to them -- two grid
+  // barriers later -- every slot is zero again: the speculative reads of
+  // grid_wait_box rely on it
+  auto zero_box = [&]() {
+    for (int i = tid; i < cnt; i += nthr) __stcg(&box[i], 0ull);
+  };
   if (cnt <= (MODE == MODE_SORT ? kFastDesc : 32) &&
-      phase_b_fast<MODE, RSM>(a, sm, k, t, cb0, cnt, spec, spec2, tail_sync))
+      phase_b_fast<MODE, RSM>(a, sm, k, t, cb0, cnt, spec, spec2, tail_sync)) {
+    zero_box();
     return;
+  }
   if (MODE == MODE_SORT && cnt > kGDesc) {
+    zero_box();
     phase_b_scan<RSM>(a, sm, scratch, k, t, b, cb0, cb1);
     return;
   }
@@ -1279,6 +1390,72 @@ __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, 
       }
     }
   }
+  zero_box();
+}
+
+// grid_wait whose polling warp also reads descriptor slots 0..63 of this
+// block's inbox (box, cap slots) in the same round trips: lane 0 polls the
+// arrivals with acquire loads, lanes 1..31 read three slots each.  On
+// return lane l of warp 0 holds slots l and l + 32 of the last poll in *d0,
+// *d1 (zero elsewhere); they are speculative -- posts can land after the
+// read that returned them -- and phase_b_spec checks them against the count.
+__device__ bool grid_wait_box(unsigned* ctr, unsigned target, int* err, unsigned long long limit_ns,
+                              const unsigned long long* box, int cap, unsigned long long* d0,
+                              unsigned long long* d1) {
+  __shared__ int s_ok;
+  unsigned long long x0 = 0ull, x1 = 0ull;
+  if (threadIdx.x < 32) {
+    const int l = threadIdx.x;
+    const int sa = l - 1, sb = l + 30, sc = l + 61;  // slots read by lane l >= 1
+    const int lim = min(cap, 64);
+    unsigned long long r0 = 0ull, r1 = 0ull, r2 = 0ull;
+    int ok = 1;
+    unsigned spins = 0;
+    unsigned long long t0 = 0;
+    for (;;) {
+      int done = 0;
+      if (l == 0) {
+        done = !before(ld_acquire_u32(ctr), target);
+      } else {
+        r0 = sa < lim ? __ldcg(box + sa) : 0ull;
+        r1 = sb < lim ? __ldcg(box + sb) : 0ull;
+        r2 = sc < lim ? __ldcg(box + sc) : 0ull;
+      }
+      if (__shfl_sync(0xffffffffu, done, 0)) break;
+      if ((++spins & 255u) == 0) {
+        int bad = 0;
+        if (l == 0) {
+          if (ld_volatile_i32(err) != 0) {
+            bad = 1;
+          } else {
+            const unsigned long long now = global_ns();
+            if (t0 == 0) t0 = now;
+            else if (now - t0 > (limit_ns ? limit_ns : kSpinTimeoutNs)) {
+              atomicCAS(err, 0, kErrTimeout);
+              bad = 1;
+            }
+          }
+        }
+        if (__shfl_sync(0xffffffffu, bad, 0)) {
+          ok = 0;
+          break;
+        }
+      }
+    }
+    // slot s sits in lane s % 31 + 1, register s / 31
+    const int sx = l, sy = l + 32;
+    const unsigned long long a0 = __shfl_sync(0xffffffffu, r0, sx % 31 + 1);
+    const unsigned long long a1 = __shfl_sync(0xffffffffu, r1, sx % 31 + 1);
+    const unsigned long long b1 = __shfl_sync(0xffffffffu, r1, sy % 31 + 1);
+    const unsigned long long b2 = __shfl_sync(0xffffffffu, r2, sy % 31 + 1);
+    x0 = sx / 31 == 0 ? a0 : a1;
+    x1 = sy / 31 == 1 ? b1 : b2;
+    if (l == 0) s_ok = ok;
+  }
+  __syncthreads();
+  *d0 = x0;
+  *d1 = x1;
+  return s_ok != 0;
 }
 
 template <int MODE, bool RSM, bool EPR>
@@ -1350,14 +1527,24 @@ __global__ void __launch_bounds__(kGThreadsMax, 1) k_tier_g(FwdArgs a) {
       for (int k = 0; k < nk; ++k)
         if (t + 1 < s_T[k])
           load_ext(a, sm.ext + (size_t)k * BS, s_samp[k], s_gb[k] + t + 1, t + 1, b);
-      if (!grid_wait(&a.ctl[0], target, a.err, a.wait_ns)) return;
-      if (MODE != MODE_ATOMIC)
-        for (int k = 0; k < nk; ++k)
-          if (t < s_T[k]) {
-            bool more = false;
-            for (int k2 = k + 1; k2 < nk; ++k2) more |= t < s_T[k2];
-            phase_b<MODE, RSM>(a, sm, scratch, k, t, b, cb0, cb1, more);
-          }
+      if (MODE != MODE_ATOMIC && nk == 1) {
+        // one sample in flight: read its inbox while waiting
+        unsigned long long d0, d1;
+        const unsigned long long* box = a.inbox + (size_t)(t & 1) * a.G + sm.ib[b];
+        if (!grid_wait_box(&a.ctl[0], target, a.err, a.wait_ns, box, sm.ib[b + 1] - sm.ib[b], &d0, &d1))
+          return;
+        if (!phase_b_spec<MODE, RSM>(a, sm, 0, t, b, cb0, d0, d1, false))
+          phase_b<MODE, RSM>(a, sm, scratch, 0, t, b, cb0, cb1, false);
+      } else {
+        if (!grid_wait(&a.ctl[0], target, a.err, a.wait_ns)) return;
+        if (MODE != MODE_ATOMIC)
+          for (int k = 0; k < nk; ++k)
+            if (t < s_T[k]) {
+              bool more = false;
+              for (int k2 = k + 1; k2 < nk; ++k2) more |= t < s_T[k2];
+              phase_b<MODE, RSM>(a, sm, scratch, k, t, b, cb0, cb1, more);
+            }
+      }
     }
     __syncthreads();
     if (tid < nk) {
@@ -1794,6 +1981,9 @@ int launch_run(Run* r, const snc_lif* lif, int mode, int path, cudaStream_t st) 
   SNCB_CUDA(cudaMemsetAsync(r->err, 0, sizeof(int), st));
   if (r->inbox_cnt)
     SNCB_CUDA(cudaMemsetAsync(r->inbox_cnt, 0, (size_t)r->Bw_cap * 2 * g->P * sizeof(int), st));
+  if (r->inbox)  // every descriptor slot starts zero (phase B keeps them so)
+    SNCB_CUDA(cudaMemsetAsync(r->inbox, 0, (size_t)r->Bw_cap * 2 * std::max(1, g->G) *
+                                               sizeof(unsigned long long), st));
   if ((r->flags & SNC_B200_RUN_RASTER) && in->raster_words)
     SNCB_CUDA(cudaMemsetAsync(r->raster, 0, (size_t)in->raster_words * sizeof(uint32_t), st));
   SNCB_CUDA(cudaEventRecord(r->ev0, st));
