@@ -649,24 +649,40 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
         const int E = base;
         if (!EP && a.s_table == 2) {
           // large chunks (kBigChunk events; staging position q = event index
-          // - e0 is the (pre, edge) order): a warp per fired row enters the
-          // row's events of the chunk in their cells' lists -- no search for
-          // an event's row -- and after one barrier every thread walks its
-          // share of the table, applying each cell's list in increasing q
-          // and clearing the entry: two barriers per 4096 events
+          // - e0 is the (pre, edge) order): every thread enters four events
+          // in their cells' lists, and after one barrier every thread walks
+          // its share of the table, applying each cell's list in increasing
+          // q and clearing the entry: two barriers per 4096 events
           for (int e0 = 0; e0 < E; e0 += kBigChunk) {
-            const int e1 = min(E, e0 + kBigChunk);
-            for (int k = warp; k < nf; k += nwarps) {
-              const int p0 = pref[k], p1 = k + 1 < nf ? pref[k + 1] : E;
-              if (p1 <= e0 || p0 >= e1) continue;  // warp-uniform
-              const int rs = fired[k] - p0;  // edge of event e: rs + e
-              for (int e = max(p0, e0) + lane; e < min(p1, e1); e += 32) {
-                const uint2 ed = a.edges[rs + e];
-                const int q = e - e0;
-                bw[q] = edge_w(ed);
-                big_insert(btab, blink, q, edge_col(ed), ring_slot(s0, edge_delay(ed), R));
+            const int ce = min(kBigChunk, E - e0);
+            // thread (warp w, lane l) stages events w * 128 + j * 32 + l,
+            // j < 4: one search for its first event's row, then the rows of
+            // the next three (32 events on) by a short forward walk; the
+            // four edge loads are issued together
+            constexpr int kPer = kBigChunk / 1024;
+            const int qb = warp * (32 * kPer) + lane;
+            int rowk = qb < ce ? upper_index(pref, nf, e0 + qb) : 0;
+            int eidx[kPer];
+#pragma unroll
+            for (int j = 0; j < kPer; ++j) {
+              const int q = qb + 32 * j;
+              eidx[j] = -1;
+              if (q < ce) {
+                const int e = e0 + q;
+                while (rowk + 1 < nf && pref[rowk + 1] <= e) ++rowk;
+                eidx[j] = fired[rowk] + (e - pref[rowk]);
               }
             }
+            uint2 ed[kPer];
+#pragma unroll
+            for (int j = 0; j < kPer; ++j) ed[j] = eidx[j] >= 0 ? a.edges[eidx[j]] : make_uint2(0u, 0u);
+#pragma unroll
+            for (int j = 0; j < kPer; ++j)
+              if (eidx[j] >= 0) {
+                const int q = qb + 32 * j;
+                bw[q] = edge_w(ed[j]);
+                big_insert(btab, blink, q, edge_col(ed[j]), ring_slot(s0, edge_delay(ed[j]), R));
+              }
             __syncthreads();
             for (int h = tid; h < kBigTable; h += nthr) {
               const unsigned ent = btab[h];
