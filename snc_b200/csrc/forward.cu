@@ -99,7 +99,7 @@ struct FwdArgs {
   float* elig;
   unsigned long long* fires;
   float gamma, trace_decay;
-  int s_table;  // tier S SORT: 1 whole-chunk cell table, 2 large chunks with a packed table
+  int s_table;  // tier S SORT: shared memory holds the whole-chunk cell table
   // deferred eligibility: psi of every ring column and step, [B][ncols][psi_T]
   // (null: eligibility accumulated in the forward into elig)
   float* psi_hist;
@@ -131,21 +131,12 @@ struct FwdArgs {
 // many list heads and one link per staged event.
 constexpr int kSTable = 2048;
 
-// Tier S SORT with large chunks (forward only): kBigChunk events per chunk,
-// a table of kBigTable packed entries (cell key << 13 | list head), a 16-bit
-// link and a weight per event -- in place of the four staging arrays.
-constexpr int kBigChunk = 4096;
-constexpr int kBigTable = 8192;
-constexpr int kBigKeyCols = (1 << 19) / 256 - 1;  // ring columns the 19-bit key holds
-
 static size_t tier_s_bytes(int N, int ncols, int R, int noc, int mode, bool eprop, int nthr,
-                           int table = 0) {
+                           bool table = false) {
   size_t words = (size_t)R * ncols + 4 * (size_t)N + (size_t)noc;
   if (mode == MODE_SORT) words += (size_t)N + 1 + 2 * (size_t)ncols + 4 * (size_t)nthr;
   if (eprop) words += (size_t)N + ncols;
-  if (mode == MODE_SORT && table == 1) words += 2 * (size_t)kSTable + nthr;
-  if (mode == MODE_SORT && table == 2)  // from st_col on: table, links, weights
-    words += kBigTable + kBigChunk / 2 + kBigChunk - 4 * (size_t)nthr;
+  if (mode == MODE_SORT && table) words += 2 * (size_t)kSTable + nthr;
   return words * 4 + 16;
 }
 
@@ -231,11 +222,13 @@ constexpr int kFirstFlag = 1 << 30;  // marks a group's first event of its colum
 // keys (column, slot) -- zeroed by the caller before staging -- holds one
 // unordered list per cell (atomicExch heads, one link per event).  The first
 // arrival at a cell owns it: alone there, it applies its event; otherwise it
-// applies the cell's list in order by repeated minimum selection.  A step's
+// collects the cell's list (kCellSort entries in registers, sorted; longer
+// lists by repeated minimum selection) and applies it in order.  A step's
 // events spread over many more cells than columns -- a column's events carry
 // different delays -- so lists are short and no thread walks a hub column's
 // whole chain.
 constexpr int kCellTable = 2 * kCountMax;  // keys, then list heads (q + 1, 0 = empty)
+constexpr int kCellSort = 8;
 static_assert(2 * kCellTable <= kGChunk, "the table lives in st_next");
 static_assert(kCellTable + kCountMax <= kGChunk, "the links live in st_col beyond the chunk");
 
@@ -278,8 +271,30 @@ __device__ __forceinline__ void cell_apply(const int* tab, const int* link, cons
   auto ord = [&](int x) -> long long {
     return KEYED ? ((long long)okey[x] << 10) | x : (long long)x;  // x < kGChunk = 1024
   };
-  // lists are short (a step's events spread over many cells): repeated
-  // minimum selection
+  long long r[kCellSort];
+#pragma unroll
+  for (int i = 0; i < kCellSort; ++i) r[i] = LLONG_MAX;
+  int p = top;
+#pragma unroll
+  for (int i = 0; i < kCellSort; ++i) {
+    if (p != 0) {
+      // insert into the sorted r (its largest entry is free)
+      r[kCellSort - 1] = ord(p - 1);
+#pragma unroll
+      for (int m = kCellSort - 1; m > 0; --m) {
+        const long long lo = min(r[m - 1], r[m]), hi = max(r[m - 1], r[m]);
+        r[m - 1] = lo;
+        r[m] = hi;
+      }
+      p = link[p - 1];
+    }
+  }
+  if (p == 0) {
+#pragma unroll
+    for (int i = 0; i < kCellSort; ++i)
+      if (r[i] != LLONG_MAX) apply_one<GLOBAL_RING>(ring, ring_stride, col0, c, sl, st_w[(int)(r[i] & 1023)]);
+    return;
+  }
   long long last = -1;
   for (;;) {
     long long best = LLONG_MAX;
@@ -289,51 +304,6 @@ __device__ __forceinline__ void cell_apply(const int* tab, const int* link, cons
     }
     if (best == LLONG_MAX) break;
     apply_one<GLOBAL_RING>(ring, ring_stride, col0, c, sl, st_w[(int)(best & 1023)]);
-    last = best;
-  }
-}
-
-// Large-chunk cell table (tier S SORT, s_table 2): one 32-bit entry per
-// cell holds its key (column * 256 + slot + 1, 19 bits) and its list head
-// (event + 1, 13 bits); links are 16-bit.
-__device__ __forceinline__ void big_insert(unsigned* tab, unsigned short* link, int q, int c, int sl) {
-  const unsigned key = (unsigned)c * 256u + (unsigned)sl + 1u;
-  const unsigned ent = (key << 13) | (unsigned)(q + 1);
-  unsigned h = (key * 2654435761u) >> (32 - 13);
-  // at most kBigChunk keys in kBigTable entries: a free or equal entry is
-  // always found; a failed CAS means another insert made progress
-  for (int probe = 0; probe < (1 << 22); ++probe) {
-    const unsigned old = *reinterpret_cast<volatile unsigned*>(&tab[h]);
-    const unsigned ok = old >> 13;
-    if (ok == 0u || ok == key) {
-      if (atomicCAS(&tab[h], old, ent) == old) {
-        link[q] = (unsigned short)(old & 8191u);  // 0: the cell's first event
-        return;
-      }
-    } else {
-      h = (h + 1u) & (kBigTable - 1);
-    }
-  }
-}
-
-// Applies the events of one table entry (after the barrier that follows the
-// inserts) to its ring cell in increasing staging index.
-__device__ __forceinline__ void big_apply(unsigned ent, const unsigned short* link, const float* w,
-                                          float* ring, int stride) {
-  const unsigned key = (ent >> 13) - 1u;
-  const int c = (int)(key >> 8), sl = (int)(key & 255u);
-  const int top = (int)(ent & 8191u);
-  if (link[top - 1] == 0) {  // one event
-    apply_one<false>(ring, stride, 0, c, sl, w[top - 1]);
-    return;
-  }
-  int last = -1;  // short lists: repeated minimum selection
-  for (;;) {
-    int best = INT_MAX;
-    for (int x = top; x != 0; x = link[x - 1])
-      if (x - 1 > last && x - 1 < best) best = x - 1;
-    if (best == INT_MAX) break;
-    apply_one<false>(ring, stride, 0, c, sl, w[best]);
     last = best;
   }
 }
@@ -511,14 +481,8 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
   // SORT with a.s_table: the per-cell table for whole chunks (kSTable keys,
   // kSTable list heads, CH links)
   int* ctab = reinterpret_cast<int*>(EP ? psi + nc : tr);
-  if (MODE == MODE_SORT && a.s_table == 1)
+  if (MODE == MODE_SORT && a.s_table)
     for (int i = tid; i < 2 * kSTable; i += nthr) ctab[i] = 0;  // ordered by the loop's first barrier
-  // s_table 2: the packed table, links and weights from st_col on
-  unsigned* btab = reinterpret_cast<unsigned*>(st_col);
-  unsigned short* blink = reinterpret_cast<unsigned short*>(btab + kBigTable);
-  float* bw = reinterpret_cast<float*>(blink + kBigChunk);
-  if (MODE == MODE_SORT && !EP && a.s_table == 2)
-    for (int i = tid; i < kBigTable; i += nthr) btab[i] = 0u;
 
   for (;;) {
     if (tid == 0) s_q = (int)atomicAdd(&a.ctl[1], 1u);
@@ -647,52 +611,7 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
         }
         __syncthreads();
         const int E = base;
-        if (!EP && a.s_table == 2) {
-          // large chunks (kBigChunk events; staging position q = event index
-          // - e0 is the (pre, edge) order): every thread enters four events
-          // in their cells' lists, and after one barrier every thread walks
-          // its share of the table, applying each cell's list in increasing
-          // q and clearing the entry: two barriers per 4096 events
-          for (int e0 = 0; e0 < E; e0 += kBigChunk) {
-            const int ce = min(kBigChunk, E - e0);
-            // thread (warp w, lane l) stages events w * 128 + j * 32 + l,
-            // j < 4: one search for its first event's row, then the rows of
-            // the next three (32 events on) by a short forward walk; the
-            // four edge loads are issued together
-            constexpr int kPer = kBigChunk / 1024;
-            const int qb = warp * (32 * kPer) + lane;
-            int rowk = qb < ce ? upper_index(pref, nf, e0 + qb) : 0;
-            int eidx[kPer];
-#pragma unroll
-            for (int j = 0; j < kPer; ++j) {
-              const int q = qb + 32 * j;
-              eidx[j] = -1;
-              if (q < ce) {
-                const int e = e0 + q;
-                while (rowk + 1 < nf && pref[rowk + 1] <= e) ++rowk;
-                eidx[j] = fired[rowk] + (e - pref[rowk]);
-              }
-            }
-            uint2 ed[kPer];
-#pragma unroll
-            for (int j = 0; j < kPer; ++j) ed[j] = eidx[j] >= 0 ? a.edges[eidx[j]] : make_uint2(0u, 0u);
-#pragma unroll
-            for (int j = 0; j < kPer; ++j)
-              if (eidx[j] >= 0) {
-                const int q = qb + 32 * j;
-                bw[q] = edge_w(ed[j]);
-                big_insert(btab, blink, q, edge_col(ed[j]), ring_slot(s0, edge_delay(ed[j]), R));
-              }
-            __syncthreads();
-            for (int h = tid; h < kBigTable; h += nthr) {
-              const unsigned ent = btab[h];
-              if (ent == 0u) continue;
-              big_apply(ent, blink, bw, ring, nc);
-              btab[h] = 0u;
-            }
-            __syncthreads();
-          }
-        } else if (a.s_table) {
+        if (a.s_table) {
           // per-cell apply of whole chunks (CH = blockDim.x: thread q stages
           // event q of the chunk and enters it in its cell's list; staging
           // order is the (pre, edge) order)
@@ -1175,107 +1094,6 @@ __device__ bool phase_b_fast(const FwdArgs& a, const GSmem& sm, int k, int t, in
   return true;
 }
 
-// Phase B for a step whose descriptors warp 0 read while it waited on the
-// grid barrier (grid_wait_box; lane l holds slots l and l + 32, zero where it
-// saw none).  Slots are zero until posted and zeroed again once consumed, so
-// the leading run of non-zero slots is a prefix of this step's descriptors:
-// its events' edges are requested at once, while thread 0 reads the count in
-// the same round trip.  When the count equals the prefix (the common case)
-// the step is applied as in phase_b_fast; otherwise -- a post the wait did
-// not see, or more events than one per thread -- nothing has been applied
-// and false sends the step to the regular path.
-template <int MODE, bool RSM>
-__device__ bool phase_b_spec(const FwdArgs& a, const GSmem& sm, int k, int t, int b, int cb0,
-                             unsigned long long d0, unsigned long long d1, bool tail_sync) {
-  __shared__ int s_E, s_cs, s_cnt;
-  const int tid = threadIdx.x, nthr = blockDim.x;
-  const int par = t & 1;
-  int* cntp = a.inbox_cnt + ((size_t)k * 2 + par) * a.P + b;
-  unsigned long long* box = a.inbox + ((size_t)k * 2 + par) * a.G + sm.ib[b];
-  int* tab = reinterpret_cast<int*>(sm.desc);
-  constexpr int kMax = kFastDesc;
-  int cnt_reg = 0;
-  if (tid == 0) cnt_reg = __ldcg(cntp);  // used after the next barrier
-  if (tid < 32) {
-    const unsigned m0 = __ballot_sync(0xffffffffu, d0 != 0ull), m1 = __ballot_sync(0xffffffffu, d1 != 0ull);
-    int cs = m0 != 0xffffffffu ? __ffs(~m0) - 1 : 32 + (m1 != 0xffffffffu ? __ffs(~m1) - 1 : 32);
-    cs = min(cs, kMax);
-    const int l0 = tid < cs ? (int)(d0 & 0xffffffffu) : 0;
-    const int l1 = tid + 32 < cs ? (int)(d1 & 0xffffffffu) : 0;
-    int i0 = l0, i1 = l1;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y0 = __shfl_up_sync(0xffffffffu, i0, o), y1 = __shfl_up_sync(0xffffffffu, i1, o);
-      if (tid >= o) {
-        i0 += y0;
-        i1 += y1;
-      }
-    }
-    const int t0 = __shfl_sync(0xffffffffu, i0, 31);
-    if (tid < cs) {
-      sm.dsort[tid] = d0;
-      sm.seg_p[tid] = i0 - l0;
-    }
-    if (tid + 32 < cs) {
-      sm.dsort[tid + 32] = d1;
-      sm.seg_p[tid + 32] = t0 + i1 - l1;
-    }
-    if (tid == 31) {
-      s_E = t0 + i1;
-      s_cs = cs;
-    }
-  }
-  if (MODE == MODE_SORT)
-    for (int i = tid; i < 2 * 2 * kFastMax; i += nthr) tab[i] = 0;
-  __syncthreads();
-  const int E = s_E, cs = s_cs;
-  const bool fits = E <= nthr && (MODE != MODE_SORT || E <= kFastMax);  // block-uniform
-  const int q = tid;
-  int edge = 0;
-  uint2 ed = make_uint2(0u, 0u);
-  if (fits && q < E) {
-    const int d = upper_index(sm.seg_p, cs, q);
-    edge = (int)(sm.dsort[d] >> 32) + (q - sm.seg_p[d]);
-    ed = a.gedges[edge];
-  }
-  if (tid == 0) s_cnt = cnt_reg;
-  __syncthreads();
-  const int cnt = s_cnt;
-  if (!fits || cnt != cs) return false;
-  if (cnt == 0) return true;
-  // consumed: the slots and the count are cleared for step t + 2
-  if (tid < cnt) __stcg(&box[tid], 0ull);
-  if (tid == 0) __stcg(cntp, 0);
-  const int R = a.R, s0 = t % R;
-  float* rb = ring_base<RSM>(a, sm, k);
-  const int stride = RSM ? a.BS : a.ncols;
-  const int col0 = RSM ? 0 : cb0;
-  if (MODE == MODE_BUCKET) {
-    if (q < E) {
-      const int cidx = RSM ? edge_col(ed) - cb0 : edge_col(ed);
-      atomicAdd(&rb[(size_t)ring_slot(s0, edge_delay(ed), R) * stride + cidx], edge_w(ed));
-    }
-    if (tail_sync) __syncthreads();
-    return true;
-  }
-  int c = 0, sl = 0;
-  unsigned h = 0;
-  bool first = false;
-  if (q < E) {
-    sl = ring_slot(s0, edge_delay(ed), R);
-    c = edge_col(ed) - cb0;
-    sm.st_w[q] = edge_w(ed);
-    sm.st_slot[q] = edge;  // order key
-    h = cell_insert<2 * kFastMax>(tab, sm.st_col, q, c, sl, &first);
-  }
-  __syncthreads();
-  if (first)
-    cell_apply<!RSM, true, 2 * kFastMax>(tab, sm.st_col, sm.st_slot, sm.st_w, h, q, c, sl, rb, stride,
-                                         col0);
-  if (tail_sync) __syncthreads();
-  return true;
-}
-
 // Phase B (BUCKET / SORT): as owner of the ring columns of block b, expand
 // this step's inbox descriptors and accumulate them into the block's ring
 // slice -- unordered (BUCKET) or per ring cell in (pre, edge) order (SORT).
@@ -1295,9 +1113,9 @@ __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, 
   const int par = t & 1;
   const int s0 = t % R;
   int* cntp = a.inbox_cnt + ((size_t)k * 2 + par) * a.P + b;
-  unsigned long long* box = a.inbox + ((size_t)k * 2 + par) * a.G + sm.ib[b];
+  const unsigned long long* box = a.inbox + ((size_t)k * 2 + par) * a.G + sm.ib[b];
   // read the first descriptor slots in the same round trip as the count
-  // (slots beyond the count are zero)
+  // (slots beyond the count hold stale descriptors and are ignored)
   const int cap = sm.ib[b + 1] - sm.ib[b];
   unsigned long long spec = 0, spec2 = 0;
   if (tid < kGDesc && tid < cap) spec = __ldcg(&box[tid]);
@@ -1310,20 +1128,10 @@ __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, 
   __syncthreads();
   const int cnt = s_cnt;
   if (cnt == 0) return;
-  // the slots this step filled are zeroed once read (by then every read of
-  // them is done), so that before the next posts to them -- two grid
-  // barriers later -- every slot is zero again: the speculative reads of
-  // grid_wait_box rely on it
-  auto zero_box = [&]() {
-    for (int i = tid; i < cnt; i += nthr) __stcg(&box[i], 0ull);
-  };
   if (cnt <= (MODE == MODE_SORT ? kFastDesc : 32) &&
-      phase_b_fast<MODE, RSM>(a, sm, k, t, cb0, cnt, spec, spec2, tail_sync)) {
-    zero_box();
+      phase_b_fast<MODE, RSM>(a, sm, k, t, cb0, cnt, spec, spec2, tail_sync))
     return;
-  }
   if (MODE == MODE_SORT && cnt > kGDesc) {
-    zero_box();
     phase_b_scan<RSM>(a, sm, scratch, k, t, b, cb0, cb1);
     return;
   }
@@ -1406,72 +1214,6 @@ __device__ void phase_b(const FwdArgs& a, const GSmem& sm, int* scratch, int k, 
       }
     }
   }
-  zero_box();
-}
-
-// grid_wait whose polling warp also reads descriptor slots 0..63 of this
-// block's inbox (box, cap slots) in the same round trips: lane 0 polls the
-// arrivals with acquire loads, lanes 1..31 read three slots each.  On
-// return lane l of warp 0 holds slots l and l + 32 of the last poll in *d0,
-// *d1 (zero elsewhere); they are speculative -- posts can land after the
-// read that returned them -- and phase_b_spec checks them against the count.
-__device__ bool grid_wait_box(unsigned* ctr, unsigned target, int* err, unsigned long long limit_ns,
-                              const unsigned long long* box, int cap, unsigned long long* d0,
-                              unsigned long long* d1) {
-  __shared__ int s_ok;
-  unsigned long long x0 = 0ull, x1 = 0ull;
-  if (threadIdx.x < 32) {
-    const int l = threadIdx.x;
-    const int sa = l - 1, sb = l + 30, sc = l + 61;  // slots read by lane l >= 1
-    const int lim = min(cap, 64);
-    unsigned long long r0 = 0ull, r1 = 0ull, r2 = 0ull;
-    int ok = 1;
-    unsigned spins = 0;
-    unsigned long long t0 = 0;
-    for (;;) {
-      int done = 0;
-      if (l == 0) {
-        done = !before(ld_acquire_u32(ctr), target);
-      } else {
-        r0 = sa < lim ? __ldcg(box + sa) : 0ull;
-        r1 = sb < lim ? __ldcg(box + sb) : 0ull;
-        r2 = sc < lim ? __ldcg(box + sc) : 0ull;
-      }
-      if (__shfl_sync(0xffffffffu, done, 0)) break;
-      if ((++spins & 255u) == 0) {
-        int bad = 0;
-        if (l == 0) {
-          if (ld_volatile_i32(err) != 0) {
-            bad = 1;
-          } else {
-            const unsigned long long now = global_ns();
-            if (t0 == 0) t0 = now;
-            else if (now - t0 > (limit_ns ? limit_ns : kSpinTimeoutNs)) {
-              atomicCAS(err, 0, kErrTimeout);
-              bad = 1;
-            }
-          }
-        }
-        if (__shfl_sync(0xffffffffu, bad, 0)) {
-          ok = 0;
-          break;
-        }
-      }
-    }
-    // slot s sits in lane s % 31 + 1, register s / 31
-    const int sx = l, sy = l + 32;
-    const unsigned long long a0 = __shfl_sync(0xffffffffu, r0, sx % 31 + 1);
-    const unsigned long long a1 = __shfl_sync(0xffffffffu, r1, sx % 31 + 1);
-    const unsigned long long b1 = __shfl_sync(0xffffffffu, r1, sy % 31 + 1);
-    const unsigned long long b2 = __shfl_sync(0xffffffffu, r2, sy % 31 + 1);
-    x0 = sx / 31 == 0 ? a0 : a1;
-    x1 = sy / 31 == 1 ? b1 : b2;
-    if (l == 0) s_ok = ok;
-  }
-  __syncthreads();
-  *d0 = x0;
-  *d1 = x1;
-  return s_ok != 0;
 }
 
 template <int MODE, bool RSM, bool EPR>
@@ -1543,24 +1285,14 @@ __global__ void __launch_bounds__(kGThreadsMax, 1) k_tier_g(FwdArgs a) {
       for (int k = 0; k < nk; ++k)
         if (t + 1 < s_T[k])
           load_ext(a, sm.ext + (size_t)k * BS, s_samp[k], s_gb[k] + t + 1, t + 1, b);
-      if (MODE != MODE_ATOMIC && nk == 1) {
-        // one sample in flight: read its inbox while waiting
-        unsigned long long d0, d1;
-        const unsigned long long* box = a.inbox + (size_t)(t & 1) * a.G + sm.ib[b];
-        if (!grid_wait_box(&a.ctl[0], target, a.err, a.wait_ns, box, sm.ib[b + 1] - sm.ib[b], &d0, &d1))
-          return;
-        if (!phase_b_spec<MODE, RSM>(a, sm, 0, t, b, cb0, d0, d1, false))
-          phase_b<MODE, RSM>(a, sm, scratch, 0, t, b, cb0, cb1, false);
-      } else {
-        if (!grid_wait(&a.ctl[0], target, a.err, a.wait_ns)) return;
-        if (MODE != MODE_ATOMIC)
-          for (int k = 0; k < nk; ++k)
-            if (t < s_T[k]) {
-              bool more = false;
-              for (int k2 = k + 1; k2 < nk; ++k2) more |= t < s_T[k2];
-              phase_b<MODE, RSM>(a, sm, scratch, k, t, b, cb0, cb1, more);
-            }
-      }
+      if (!grid_wait(&a.ctl[0], target, a.err, a.wait_ns)) return;
+      if (MODE != MODE_ATOMIC)
+        for (int k = 0; k < nk; ++k)
+          if (t < s_T[k]) {
+            bool more = false;
+            for (int k2 = k + 1; k2 < nk; ++k2) more |= t < s_T[k2];
+            phase_b<MODE, RSM>(a, sm, scratch, k, t, b, cb0, cb1, more);
+          }
     }
     __syncthreads();
     if (tid < nk) {
@@ -1710,26 +1442,9 @@ static int launch_tier_s_kernel(const Graph* g, int B, const FwdArgs& a_in, cuda
   int per_sm = 0;
   SNCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tier_s<MODE, EP>, nthr, smem));
   a.s_table = 0;
-  if (MODE == MODE_SORT && !EP && g->ncols <= kBigKeyCols) {
-    // large chunks when they fit without costing a CTA per SM
-    const size_t smem_b = tier_s_bytes(g->N, g->ncols, g->R, a.noc, MODE, EP, nthr, 2);
-    int per_sm_b = 0;
-    if ((int)smem_b <= optin_smem() &&
-        cudaFuncSetAttribute(k_tier_s<MODE, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b) ==
-            cudaSuccess &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_b, k_tier_s<MODE, EP>, nthr, smem_b) ==
-            cudaSuccess &&
-        per_sm_b >= per_sm && per_sm_b >= 1) {
-      smem = smem_b;
-      a.s_table = 2;
-    } else {
-      cudaGetLastError();
-      SNCB_CUDA(cudaFuncSetAttribute(k_tier_s<MODE, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    }
-  }
-  if (MODE == MODE_SORT && a.s_table == 0) {
+  if (MODE == MODE_SORT) {
     // the per-cell table when it fits without costing a CTA per SM
-    const size_t smem_t = tier_s_bytes(g->N, g->ncols, g->R, a.noc, MODE, EP, nthr, 1);
+    const size_t smem_t = tier_s_bytes(g->N, g->ncols, g->R, a.noc, MODE, EP, nthr, true);
     int per_sm_t = 0;
     if ((int)smem_t <= optin_smem() &&
         cudaFuncSetAttribute(k_tier_s<MODE, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t) ==
@@ -1997,9 +1712,6 @@ int launch_run(Run* r, const snc_lif* lif, int mode, int path, cudaStream_t st) 
   SNCB_CUDA(cudaMemsetAsync(r->err, 0, sizeof(int), st));
   if (r->inbox_cnt)
     SNCB_CUDA(cudaMemsetAsync(r->inbox_cnt, 0, (size_t)r->Bw_cap * 2 * g->P * sizeof(int), st));
-  if (r->inbox)  // every descriptor slot starts zero (phase B keeps them so)
-    SNCB_CUDA(cudaMemsetAsync(r->inbox, 0, (size_t)r->Bw_cap * 2 * std::max(1, g->G) *
-                                               sizeof(unsigned long long), st));
   if ((r->flags & SNC_B200_RUN_RASTER) && in->raster_words)
     SNCB_CUDA(cudaMemsetAsync(r->raster, 0, (size_t)in->raster_words * sizeof(uint32_t), st));
   SNCB_CUDA(cudaEventRecord(r->ev0, st));
