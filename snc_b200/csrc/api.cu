@@ -293,27 +293,42 @@ static int create_run(const Graph* g, const Inputs* in, int flags, Run* r) {
 }
 
 int fetch_run(Run* r, float* logits, int64_t* spikes, int64_t* events, uint32_t* raster,
-                     float* v_final, snc_run_stats* stats) {
+              float* v_final, snc_run_stats* stats, const int* d_sched_err, int* sched_err) {
   const Graph* g = r->g;
   const Inputs* in = r->in;
   SNCB_CUDA(cudaEventSynchronize(r->ev1));
-  int err = 0;
-  SNCB_CUDA(cudaMemcpy(&err, r->err, sizeof(int), cudaMemcpyDeviceToHost));
   float ms = 0.f;
   SNCB_CUDA(cudaEventElapsedTime(&ms, r->ev0, r->ev1));
   r->last_ms = ms;
   const int B = in->B, noc = std::max(1, g->noc);
-  std::vector<int> counts((size_t)std::max(1, B) * noc);
-  std::vector<unsigned long long> sp(std::max(1, B)), evn(std::max(1, B));
+  const bool ro = logits && r->ro_decay >= 0.f && r->ro_logits && B > 0;
+  // pinned block: err, schedule err | spikes [B] | events [B] | counts [B][noc] | readout [B][noc]
+  const size_t Bn = (size_t)std::max(0, B);
+  const size_t o_sp = 8, o_ev = o_sp + 8 * Bn, o_cnt = o_ev + 8 * Bn;
+  const size_t o_lg = o_cnt + 4 * Bn * noc, total = o_lg + (ro ? 4 * Bn * noc : 0);
+  int rc;
+  if ((rc = r->fetch_img.reserve(total))) return rc;
+  unsigned char* h = r->fetch_img.p;
+  std::memset(h, 0, 8);
+  const cudaStream_t s0 = cudaStreamPerThread;
+  SNCB_CUDA(cudaMemcpyAsync(h, r->err, 4, cudaMemcpyDeviceToHost, s0));
+  if (d_sched_err) SNCB_CUDA(cudaMemcpyAsync(h + 4, d_sched_err, 4, cudaMemcpyDeviceToHost, s0));
   if (B > 0) {
-    SNCB_CUDA(cudaMemcpy(counts.data(), r->counts, (size_t)B * noc * sizeof(int), cudaMemcpyDeviceToHost));
-    SNCB_CUDA(cudaMemcpy(sp.data(), r->spikes, (size_t)B * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
-    SNCB_CUDA(cudaMemcpy(evn.data(), r->events, (size_t)B * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    SNCB_CUDA(cudaMemcpyAsync(h + o_sp, r->spikes, 8 * Bn, cudaMemcpyDeviceToHost, s0));
+    SNCB_CUDA(cudaMemcpyAsync(h + o_ev, r->events, 8 * Bn, cudaMemcpyDeviceToHost, s0));
+    SNCB_CUDA(cudaMemcpyAsync(h + o_cnt, r->counts, 4 * Bn * noc, cudaMemcpyDeviceToHost, s0));
+    if (ro) SNCB_CUDA(cudaMemcpyAsync(h + o_lg, r->ro_logits, 4 * Bn * noc, cudaMemcpyDeviceToHost, s0));
   }
-  if (logits && r->ro_decay >= 0.f && r->ro_logits && B > 0) {
+  SNCB_CUDA(cudaStreamSynchronize(s0));
+  int err = 0;
+  std::memcpy(&err, h, 4);
+  if (sched_err) std::memcpy(sched_err, h + 4, 4);
+  const int* counts = reinterpret_cast<const int*>(h + o_cnt);
+  const unsigned long long* sp = reinterpret_cast<const unsigned long long*>(h + o_sp);
+  const unsigned long long* evn = reinterpret_cast<const unsigned long long*>(h + o_ev);
+  if (ro) {
     // leaky readout units: their potentials over the sample's steps
-    std::vector<float> lg((size_t)B * noc);
-    SNCB_CUDA(cudaMemcpy(lg.data(), r->ro_logits, lg.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    const float* lg = reinterpret_cast<const float*>(h + o_lg);
     for (int b = 0; b < B; ++b)
       for (int c = 0; c < g->noc; ++c) logits[(size_t)b * g->noc + c] = lg[(size_t)b * noc + c];
   } else if (logits) {

@@ -173,6 +173,9 @@ struct Run {
   unsigned long long* events = nullptr;  // [B]
   uint32_t* raster = nullptr;            // [raster_words]
   float* vfinal = nullptr;               // [B][N]
+  // the small results (error words, counters, logits) come back through one
+  // pinned block: asynchronous copies and a single synchronisation
+  HostImage fetch_img{true};
   // control
   int* err = nullptr;
   unsigned* ctl = nullptr;  // [0] barrier counter, [1] work-queue counter
@@ -289,8 +292,12 @@ int oneshot_forward(const Graph* g, const snc_input_event* ev, size_t n_ev, int 
 void free_oneshot(const Graph* g);
 
 // api.cu
+// Waits for the run and copies its results out.  d_sched_err, when given,
+// is the schedule builder's overflow word, read in the same batch of copies
+// into *sched_err.
 int fetch_run(Run* r, float* logits, int64_t* spikes, int64_t* events, uint32_t* raster,
-              float* v_final, snc_run_stats* stats);
+              float* v_final, snc_run_stats* stats, const int* d_sched_err = nullptr,
+              int* sched_err = nullptr);
 void free_run(Run* r);
 
 // forward.cu

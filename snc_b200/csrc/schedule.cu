@@ -789,9 +789,9 @@ int oneshot_forward(const Graph* g, const snc_input_event* ev, size_t n_ev, int 
     ws->B_cap = Bc;
   }
   if ((rc = launch_run(&r, lif, mode, path, ws->stream))) return rc;
-  rc = fetch_run(&r, logits, spikes, events_out, nullptr, nullptr, stats);
   int err = 0;
-  if (cudaMemcpy(&err, in.d_err, 4, cudaMemcpyDeviceToHost) == cudaSuccess && err && !rc) {
+  rc = fetch_run(&r, logits, spikes, events_out, nullptr, nullptr, stats, in.d_err, &err);
+  if (err && !rc) {
     set_error("schedule entries exceeded their bound");
     rc = SNC_B200_EOVERFLOW;
     if (stats) stats->overflow = 1;

@@ -7,8 +7,11 @@ Samples are independent under a frozen graph (include/snc/cuda_trainer.hpp:
     (snc_b200_eprop_gradient), one all-reduce (sum) adds the shards, every
     rank applies the same update with the global batch size
     (snc_b200_eprop_apply) -- the weights stay identical on all ranks;
-  * BPTT: SNNFunction returns ordinary gradients, so the models work under
-    torch.nn.parallel.DistributedDataParallel unchanged.
+  * BPTT: SNNFunction returns ordinary autograd gradients; DataParallelBPTT
+    computes each rank's shard gradient of the summed loss, adds the shards
+    with one all-reduce of a single flat buffer and divides by the global
+    batch, so uneven shards give the gradient of the global mean loss (DDP's
+    averaging over ranks assumes equal shards).
 The collective is torch.distributed (NCCL over NVLink on GPUs, gloo in the
 CPU tests).  Remote data always arrives in local memory through NCCL; no
 kernel here reads a peer's memory.
@@ -70,6 +73,67 @@ class DataParallelEprop:
             dist.all_reduce(grad, op=dist.ReduceOp.SUM, group=self.group)
         self.session.apply(grad, int(np.asarray(steps).shape[0]))
         return out
+
+
+def shard_gradient(model, loss_fn, inputs, targets, batch_dim: int, rank: int, world: int):
+    """This rank's share of one BPTT minibatch: the gradient of the SUMMED
+    loss over its contiguous block of samples (shard_bounds), flattened over
+    model.parameters() in order (zeros for a parameter without a gradient or
+    an empty shard), and the summed loss.  loss_fn(model, x, y) returns the
+    sum of per-sample losses of its samples."""
+    import torch
+    B = inputs.shape[batch_dim]
+    lo, hi = shard_bounds(B, rank, world)
+    params = [p for p in model.parameters()]
+    for p in params:
+        p.grad = None
+    loss = torch.zeros((), dtype=torch.float64, device=params[0].device)
+    if hi > lo:
+        x = inputs.narrow(batch_dim, lo, hi - lo)
+        y = targets[lo:hi]
+        ls = loss_fn(model, x, y)
+        ls.backward()
+        loss = ls.detach().to(torch.float64)
+    flat = torch.cat([(p.grad if p.grad is not None else torch.zeros_like(p)).reshape(-1).float()
+                      for p in params])
+    return flat, loss
+
+
+class DataParallelBPTT:
+    """One BPTT update over a global minibatch split across ranks: every rank
+    computes its shard's gradient of the summed loss (shard_gradient), one
+    all-reduce (sum) of the flat gradient and the loss adds the shards, the
+    sum is divided by the global batch and written back to the parameters'
+    .grad, and every rank takes the same optimizer step -- parameters stay
+    identical on all ranks.  batch_dim is the inputs' sample dimension (1 for
+    the [T, B, ...] spike tensors of DelayedSNN, 0 for SpikingLM's [B, T]
+    tokens); targets are indexed by sample along dimension 0."""
+
+    def __init__(self, model, optimizer, loss_fn, batch_dim: int, group=None):
+        self.model, self.optimizer, self.loss_fn = model, optimizer, loss_fn
+        self.batch_dim, self.group = batch_dim, group
+
+    def step(self, inputs, targets):
+        import torch
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            world, rank = dist.get_world_size(self.group), dist.get_rank(self.group)
+        else:
+            world, rank = 1, 0
+        B = inputs.shape[self.batch_dim]
+        flat, loss = shard_gradient(self.model, self.loss_fn, inputs, targets, self.batch_dim, rank,
+                                    world)
+        buf = torch.cat([flat, loss.float().reshape(1)])
+        if world > 1:
+            dist.all_reduce(buf, op=dist.ReduceOp.SUM, group=self.group)
+        buf /= float(B)
+        off = 0
+        for p in self.model.parameters():
+            n = p.numel()
+            p.grad = buf[off:off + n].view_as(p).to(p.dtype).clone()
+            off += n
+        self.optimizer.step()
+        return float(buf[-1])
 
 
 def part_block_bounds(num_blocks: int, rank: int, world: int):

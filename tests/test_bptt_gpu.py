@@ -341,3 +341,29 @@ def test_char_lm_bench_shape_gradients():
                                                          net.w_rec.detach(), ext, 16, 5)
     assert gw_max <= 1e-4 and gw_el <= 1e-4, (gw_max, gw_el)
     assert ge_max <= 1e-4 and ge_el <= 1e-4, (ge_max, ge_el)
+
+
+def test_shard_gradients_add_up_to_the_full_batch():
+    """Sample-sharded BPTT (snc_b200.parallel.shard_gradient, the per-rank
+    half of DataParallelBPTT) with the custom kernels: the shards' gradients
+    of the summed loss over 2 and 3 uneven shards add up to the whole batch's
+    gradient (samples are independent; only the dW summation order across
+    the batch differs)."""
+    from snc_b200 import parallel as PAR
+    d = W.random_graph(8, n_in=20, n_hid=60, n_out=6, max_delay=4)
+    ro_ids = np.nonzero(np.asarray(d.role) == 2)[0]
+    net = BP.DelayedSNN(d.num_neurons, d.pre_ids(), d.post_ids, d.delays, 20, ro_ids, 3, thr=1.0,
+                        decay=0.9, surrogate_scale=25.0, ckpt_every=6, seed=2).to(DEV)
+    T, B = 24, 7
+    x = (torch.rand(T, B, 20, generator=torch.Generator().manual_seed(4)) < 0.3).float().to(DEV)
+    y = torch.as_tensor(np.random.default_rng(1).integers(0, 3, B)).to(DEV)
+
+    def loss_fn(m, xs, ys):
+        return torch.nn.functional.cross_entropy(m(xs), ys, reduction="sum")
+
+    full, lf = PAR.shard_gradient(net, loss_fn, x, y, 1, 0, 1)
+    assert float(full.abs().max()) > 0
+    for world in (2, 3):
+        parts = [PAR.shard_gradient(net, loss_fn, x, y, 1, r, world) for r in range(world)]
+        rel_close(sum(g for g, _ in parts).cpu(), full.cpu(), 1e-5)
+        assert abs(float(sum(l for _, l in parts)) - float(lf)) <= 1e-5 * abs(float(lf))

@@ -154,3 +154,89 @@ def test_part_block_bounds_cover_the_blocks():
             spans = [PAR.part_block_bounds(P, r, world) for r in range(world)]
             assert spans[0][0] == 0 and spans[-1][1] == P
             assert all(a[1] == b[0] for a, b in zip(spans, spans[1:]))
+
+
+# ---- sample-sharded BPTT (DataParallelBPTT on gloo ranks) ----------------------
+
+class _RefDelayedSNN(torch.nn.Module):
+    """CPU stand-in for snc_b200.bptt.DelayedSNN: the autograd restatement
+    of the delayed spiking core and its leaky readout (the kernels need a
+    GPU; the sharding, all-reduce and update logic under test do not)."""
+
+    def __init__(self, g, n_in, ro_ids, n_class):
+        super().__init__()
+        from oracle import bptt_ref as BR
+        self.BR = BR
+        gen = torch.Generator().manual_seed(5)
+        self.w = torch.nn.Parameter((torch.rand(g.num_synapses, generator=gen) * 2 - 1) * 0.6)
+        self.readout = torch.nn.Linear(len(ro_ids), n_class)
+        with torch.no_grad():
+            self.readout.weight.copy_(torch.randn(self.readout.weight.shape, generator=gen) * 0.3)
+            self.readout.bias.copy_(torch.randn(n_class, generator=gen) * 0.1)
+        self.N, self.n_in = g.num_neurons, n_in
+        self.pre = torch.as_tensor(g.pre_ids()).long()
+        self.post = torch.as_tensor(g.post_ids).long()
+        self.delays = torch.as_tensor(g.delays).long()
+        self.ro_ids = torch.as_tensor(ro_ids).long()
+
+    def forward(self, spikes_in):
+        T, B, _ = spikes_in.shape
+        ext = torch.zeros(T, B, self.N)
+        ext[:, :, :self.n_in] = spikes_in
+        s = self.BR.core_forward(self.w, ext, self.pre, self.post, self.delays, 1.0, 0.9, 25.0)
+        return self.BR.leaky_readout(s, self.readout.weight, self.readout.bias, self.ro_ids, 0.9)
+
+
+def bptt_case():
+    g = W.random_graph(8, n_in=12, n_hid=30, n_out=4, max_delay=3)
+    ro_ids = np.nonzero(np.asarray(g.role) == 2)[0]
+    T, B = 16, 5
+    x = (torch.rand(T, B, 12, generator=torch.Generator().manual_seed(3)) < 0.35).float()
+    y = torch.as_tensor(np.random.default_rng(2).integers(0, 3, B))
+    return g, ro_ids, x, y
+
+
+def _bptt_loss(m, xs, ys):
+    return torch.nn.functional.cross_entropy(m(xs), ys, reduction="sum")
+
+
+def _bptt_worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        g, ro_ids, x, y = bptt_case()
+        torch.manual_seed(0)
+        m = _RefDelayedSNN(g, 12, ro_ids, 3)
+        opt = torch.optim.SGD(m.parameters(), lr=0.5)
+        loss = PAR.DataParallelBPTT(m, opt, _bptt_loss, batch_dim=1).step(x, y)
+        torch.save({"w": m.w.detach(), "rw": m.readout.weight.detach(),
+                    "rb": m.readout.bias.detach(), "loss": loss}, os.path.join(out, f"b{rank}.pt"))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_data_parallel_bptt_gloo_world2(tmp_path):
+    """Two gloo ranks take one SGD step on uneven shards (3 + 2 samples) of a
+    5-sample minibatch: both end with identical parameters, equal (up to
+    float summation order) to one step on the whole batch's mean loss."""
+    port = 29900 + (os.getpid() % 1000)
+    mp.start_processes(_bptt_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    r0 = torch.load(tmp_path / "b0.pt")
+    r1 = torch.load(tmp_path / "b1.pt")
+    for k in ("w", "rw", "rb"):
+        assert torch.equal(r0[k], r1[k])
+    g, ro_ids, x, y = bptt_case()
+    torch.manual_seed(0)
+    m = _RefDelayedSNN(g, 12, ro_ids, 3)
+    w0 = m.w.detach().clone()
+    opt = torch.optim.SGD(m.parameters(), lr=0.5)
+    loss = torch.nn.functional.cross_entropy(m(x), y)
+    loss.backward()
+    opt.step()
+    assert float((m.w.detach() - w0).abs().max()) > 0
+    torch.testing.assert_close(r0["w"], m.w.detach(), rtol=1e-5, atol=1e-6)
+    torch.testing.assert_close(r0["rw"], m.readout.weight.detach(), rtol=1e-5, atol=1e-6)
+    torch.testing.assert_close(r0["rb"], m.readout.bias.detach(), rtol=1e-5, atol=1e-6)
+    assert abs(r0["loss"] - float(loss)) <= 1e-5 * abs(float(loss))
