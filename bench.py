@@ -824,7 +824,23 @@ def our_arm(args):
             traffic = None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                "kernel": "k_tier_g", "bytes_per_launch": per_launch_bytes}
+                "kernel": "k_tier_g", "bytes_per_launch": per_launch_bytes,
+                "bytes_per_launch_with_ring_rmw": per_launch_bytes + 8 * ev_n / args.steps}
+    # the atomic half: the ATOMIC delivery mode (one red.global.add.f32 per
+    # synaptic event into an L2-resident ring) against the measured rate of
+    # scattered reductions into a buffer of the ring's size
+    ra = R.Run(dg, di, cuda_graph=True)
+    timed(ra, R.MODE_ATOMIC, R.PATH_PERSISTENT, 2)
+    msa, eva, _ = timed(ra, R.MODE_ATOMIC, R.PATH_PERSISTENT, max(2, min(5, args.steps)))
+    ra.release()
+    ring_slots = (int(g.delays.max()) + 1) * g.num_neurons
+    red_peak = R.probe_red_rate(ring_slots)
+    red_ach = eva / (sum(msa) / 1e3)
+    roofline["atomic"] = {"mode": "atomic", "achieved": red_ach, "peak": red_peak, "unit": "reductions/s",
+                          "frac": red_ach / red_peak, "ms_per_launch": sum(msa) / len(msa),
+                          "reductions_per_launch": eva / len(msa),
+                          "peak_kind": f"measured here: snc_b200_probe_red_rate over {ring_slots} floats "
+                                       "(the ring's size), scattered addresses, all SMs"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_extra:

@@ -140,6 +140,14 @@ int snc_b200_inject_stall(int32_t n);
  * process that cannot call this (the reference's CLIs linked with the
  * adapter) can still be made to take its CPU fallback.  Process-wide. */
 int snc_b200_inject_alloc_failure(int64_t after);
+/* Measurement: the rate (reductions per second) at which this GPU completes
+ * float reductions to scattered addresses of a buffer of `n_slots` floats --
+ * `n_ops` reductions from an all-SM grid, each warp's lanes on unrelated
+ * words, the second of two launches timed.  The denominator of the ATOMIC
+ * delivery mode's roofline (one reduction per synaptic event into the delay
+ * ring, the reference's k_step delivery, src/runtime/cuda_backend.cu:71-75);
+ * no reference counterpart of its own. */
+int snc_b200_probe_red_rate(int64_t n_slots, int64_t n_ops, double* reds_per_s);
 
 /* ---- graph ----------------------------------------------------------------*/
 
@@ -416,6 +424,64 @@ int snc_b200_eprop_get_eligibility(snc_b200_eprop* s, float* elig);
  * per-neuron firings [N] accumulated over training minibatches. */
 int snc_b200_eprop_reset_stats(snc_b200_eprop* s);
 int snc_b200_eprop_collect_stats(snc_b200_eprop* s, int64_t* syn_deliveries, int64_t* neuron_fires);
+
+/* ---- connectome: the co-training loop's structural state (replaces
+ * snc::Connectome, include/snc/connectome.hpp:58-101, for the loop of
+ * src/training/cotrain_main.cpp:271-283) -------------------------------------
+ * A layered edge list with per-edge ages kept on the device as a CSR (rows in
+ * the reference's adjacency order), pruned and regrown there by
+ * snc_b200_connectome_update and turned into a device graph without a host
+ * round trip.  Random draws (initial jitter, fallback growth) come from the
+ * host's std::mt19937_64 through the same library distributions as the
+ * reference, so a connectome made here from the same seed evolves as the
+ * reference's does; one documented difference: among eligible synapses of
+ * equal |weight| at the K-th place the lowest CSR positions are pruned
+ * (std::nth_element leaves that choice to the library). */
+typedef struct snc_b200_connectome snc_b200_connectome;
+
+typedef struct {                /* StructConfig, connectome.hpp:33-48 */
+  int32_t grow_per_epoch;
+  int32_t delay;
+  float w_grow_init;
+  float locality_window;
+  int32_t protect_rounds;
+  int32_t max_attempts_mult;
+  int32_t reward_modulated;
+  float reward_chance;
+  float reward_floor;
+} snc_struct_config;
+
+typedef struct {                /* StructReport, connectome.hpp:50-54 */
+  int32_t pruned;
+  int32_t grown;
+  int32_t synapses;
+} snc_struct_report;
+
+/* Connectome::layered_local (connectome.cpp:14-62). */
+int snc_b200_connectome_layered_local(const int32_t* layers, int32_t num_layers,
+                                      int32_t synapse_budget, int32_t delay, float w_init,
+                                      uint64_t seed, snc_b200_connectome** out);
+int snc_b200_connectome_release(snc_b200_connectome* c);
+int snc_b200_connectome_info(const snc_b200_connectome* c, int32_t* num_neurons,
+                             int32_t* num_synapses);
+/* to_graph()'s CSR (row_ptr [N+1], post, delay), edge_weights() (signed,
+ * the same order) and the structural ages; NULL arrays are skipped. */
+int snc_b200_connectome_read(const snc_b200_connectome* c, int32_t* row_ptr, int32_t* post,
+                             int32_t* delay, float* weight, int32_t* age);
+/* set_edge_weights (connectome.cpp:112-119): the first n weights in CSR
+ * order, the rest unchanged. */
+int snc_b200_connectome_set_weights(snc_b200_connectome* c, const float* w, int64_t n);
+/* structural_update (connectome.cpp:121-219): prune the K weakest eligible
+ * synapses (K from grow_per_epoch, reward-modulated if asked), regrow one
+ * local synapse per freed post from the most active unconnected pre in its
+ * window, then fallback growth onto under-driven random posts, then age every
+ * synapse.  neuron_fires [n_fires] are the inner loop's firing counts
+ * (snc_b200_eprop_collect_stats). */
+int snc_b200_connectome_update(snc_b200_connectome* c, const int64_t* neuron_fires, int64_t n_fires,
+                               const snc_struct_config* cfg, float reward, snc_struct_report* out);
+/* to_graph (connectome.cpp:84-101) on the device: |weight|, sign +1, the
+ * layers' roles and channels. */
+int snc_b200_connectome_graph(const snc_b200_connectome* c, snc_b200_graph** out);
 
 /* ---- surrogate-gradient BPTT (replaces the autograd unrolling of the bridge,
  * python/snc/model.py:52-72, with the per-synapse delays of

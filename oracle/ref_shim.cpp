@@ -14,12 +14,14 @@
 //   snc::make_static_snc etc.  include/snc/snn_graph.hpp:118-132
 //   snc::make_synthetic        include/snc/dataset.hpp:27
 //   snc::Trainer               include/snc/trainer.hpp:59-107
+//   snc::Connectome            include/snc/connectome.hpp:58-101
 #include <cstdint>
 #include <cstring>
 #include <random>
 #include <string>
 #include <vector>
 
+#include "snc/connectome.hpp"
 #include "snc/dataset.hpp"
 #include "snc/encoders.hpp"
 #include "snc/runtime.hpp"
@@ -210,6 +212,58 @@ int64_t ref_trainer_one_sample(void* gp, int num_steps, float threshold, float d
   tr.train_epoch(d, d, epoch);
   std::memcpy(w_after, tr.weights().data(), sizeof(float) * tr.weights().size());
   return n;
+}
+
+// ---- Connectome (the co-training loop's structural state) -------------------
+
+void* ref_con_layered_local(const int32_t* layers, int n_layers, int budget, int delay, float w_init,
+                            uint64_t seed) {
+  std::vector<int> l(layers, layers + n_layers);
+  return new Connectome(Connectome::layered_local(l, budget, delay, w_init, seed));
+}
+
+void ref_con_destroy(void* h) { delete static_cast<Connectome*>(h); }
+
+int ref_con_num_synapses(void* h) { return static_cast<Connectome*>(h)->num_synapses(); }
+
+// to_graph() CSR (row_ptr [n+1], post, delay) and edge_weights() (signed).
+int ref_con_read(void* h, int32_t* row_ptr, int32_t* post, int32_t* delay, float* w_signed) {
+  auto* c = static_cast<Connectome*>(h);
+  const SNNGraph g = c->to_graph();
+  const std::vector<float> w = c->edge_weights();
+  std::memcpy(row_ptr, g.row_ptr.data(), sizeof(int32_t) * g.row_ptr.size());
+  std::memcpy(post, g.post_ids.data(), sizeof(int32_t) * g.post_ids.size());
+  std::memcpy(delay, g.delays.data(), sizeof(int32_t) * g.delays.size());
+  std::memcpy(w_signed, w.data(), sizeof(float) * w.size());
+  return g.num_neurons;
+}
+
+void ref_con_set_weights(void* h, const float* w, int n) {
+  static_cast<Connectome*>(h)->set_edge_weights(std::vector<float>(w, w + n));
+}
+
+// structural_update with the given activity and configuration; out[3] =
+// pruned, grown, synapses.
+void ref_con_update(void* h, const int64_t* fires, int n_fires, int grow_per_epoch, int delay,
+                    float w_grow_init, float locality_window, int protect_rounds,
+                    int max_attempts_mult, int reward_modulated, float reward_chance,
+                    float reward_floor, float reward, int32_t* out) {
+  ActivityStats st;
+  st.neuron_fires.assign(fires, fires + n_fires);
+  StructConfig cfg;
+  cfg.grow_per_epoch = grow_per_epoch;
+  cfg.delay = delay;
+  cfg.w_grow_init = w_grow_init;
+  cfg.locality_window = locality_window;
+  cfg.protect_rounds = protect_rounds;
+  cfg.max_attempts_mult = max_attempts_mult;
+  cfg.reward_modulated = reward_modulated != 0;
+  cfg.reward_chance = reward_chance;
+  cfg.reward_floor = reward_floor;
+  const StructReport r = static_cast<Connectome*>(h)->structural_update(st, cfg, reward);
+  out[0] = r.pruned;
+  out[1] = r.grown;
+  out[2] = r.synapses;
 }
 
 }  // extern "C"

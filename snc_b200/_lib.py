@@ -52,6 +52,17 @@ class GridGraph(C.Structure):
                 ("max_delay", C.c_int32), ("max_draws", C.c_int32), ("seed", C.c_uint64)]
 
 
+class StructConfig(C.Structure):
+    _fields_ = [("grow_per_epoch", C.c_int32), ("delay", C.c_int32), ("w_grow_init", C.c_float),
+                ("locality_window", C.c_float), ("protect_rounds", C.c_int32),
+                ("max_attempts_mult", C.c_int32), ("reward_modulated", C.c_int32),
+                ("reward_chance", C.c_float), ("reward_floor", C.c_float)]
+
+
+class StructReport(C.Structure):
+    _fields_ = [("pruned", C.c_int32), ("grown", C.c_int32), ("synapses", C.c_int32)]
+
+
 class RunStats(C.Structure):
     _fields_ = [("spikes", C.c_int64), ("synaptic_events", C.c_int64), ("overflow", C.c_int32),
                 ("ms", C.c_double)]
@@ -72,6 +83,14 @@ SIGNATURES = {
     "snc_b200_set_wait_limit": (C.c_int, [C.c_uint64]),
     "snc_b200_inject_stall": (C.c_int, [I32]),
     "snc_b200_inject_alloc_failure": (C.c_int, [C.c_int64]),
+    "snc_b200_probe_red_rate": (C.c_int, [C.c_int64, C.c_int64, P]),
+    "snc_b200_connectome_layered_local": (C.c_int, [P, I32, I32, I32, C.c_float, C.c_uint64, P]),
+    "snc_b200_connectome_release": (C.c_int, [P]),
+    "snc_b200_connectome_info": (C.c_int, [P, P, P]),
+    "snc_b200_connectome_read": (C.c_int, [P] * 6),
+    "snc_b200_connectome_set_weights": (C.c_int, [P, P, C.c_int64]),
+    "snc_b200_connectome_update": (C.c_int, [P, P, C.c_int64, P, C.c_float, P]),
+    "snc_b200_connectome_graph": (C.c_int, [P, P]),
     "snc_b200_graph_upload": (C.c_int, [P, P]),
     "snc_b200_graph_release": (C.c_int, [P]),
     "snc_b200_graph_upload_sncg": (C.c_int, [P, C.c_size_t, P]),

@@ -363,3 +363,12 @@ def autotune_lookup(dg: DeviceGraph, inputs: DeviceInputs) -> dict | None:
     """The cached autotuner choice for this graph and batch shape, or None."""
     c = _lib.LaunchConfig()
     return _shape_dict(c) if lib().snc_b200_autotune_lookup(dg.h, inputs.h, C.byref(c)) == 1 else None
+
+
+def probe_red_rate(n_slots: int, n_ops: int = 1 << 28) -> float:
+    """Reductions per second this GPU completes at scattered addresses of a
+    buffer of n_slots floats (snc_b200_probe_red_rate): the denominator of
+    the ATOMIC delivery mode's roofline."""
+    out = C.c_double()
+    check(lib().snc_b200_probe_red_rate(int(n_slots), int(n_ops), C.byref(out)), "probe_red_rate")
+    return float(out.value)
