@@ -99,7 +99,7 @@ struct FwdArgs {
   float* elig;
   unsigned long long* fires;
   float gamma, trace_decay;
-  int s_table;  // tier S SORT: shared memory holds the whole-chunk cell table
+  int s_table;  // tier S SORT: 1 the whole-chunk cell table, 2 also the cell bitmaps
   // deferred eligibility: psi of every ring column and step, [B][ncols][psi_T]
   // (null: eligibility accumulated in the forward into elig)
   float* psi_hist;
@@ -131,12 +131,17 @@ struct FwdArgs {
 // many list heads and one link per staged event.
 constexpr int kSTable = 2048;
 
+// With table == 2 four bitmaps of the ring's cells follow (two alternating
+// pairs: seen, hit more than once).
+static size_t cell_bitmap_words(int ncols, int R) { return ((size_t)R * ncols + 31) / 32; }
+
 static size_t tier_s_bytes(int N, int ncols, int R, int noc, int mode, bool eprop, int nthr,
-                           bool table = false) {
+                           int table = 0) {
   size_t words = (size_t)R * ncols + 4 * (size_t)N + (size_t)noc;
   if (mode == MODE_SORT) words += (size_t)N + 1 + 2 * (size_t)ncols + 4 * (size_t)nthr;
   if (eprop) words += (size_t)N + ncols;
   if (mode == MODE_SORT && table) words += 2 * (size_t)kSTable + nthr;
+  if (mode == MODE_SORT && table == 2) words += 4 * cell_bitmap_words(ncols, R);
   return words * 4 + 16;
 }
 
@@ -259,11 +264,10 @@ __device__ __forceinline__ unsigned cell_insert(int* tab, int* link, int q, int 
 // The owner's part (after a barrier that follows every cell_insert): apply
 // the cell's events in increasing order -- their staging index, or with
 // KEYED their order key okey[x] (unique per event) -- then x.
-template <bool GLOBAL_RING, bool KEYED, int TS>
-__device__ __forceinline__ void cell_apply(const int* tab, const int* link, const int* okey,
-                                           const float* st_w, unsigned h, int q, int c, int sl,
-                                           float* ring, int ring_stride, int col0) {
-  const int top = tab[TS + h];
+template <bool GLOBAL_RING, bool KEYED>
+__device__ __forceinline__ void cell_apply_list(int top, const int* link, const int* okey,
+                                                const float* st_w, int q, int c, int sl, float* ring,
+                                                int ring_stride, int col0) {
   if (top == q + 1) {
     apply_one<GLOBAL_RING>(ring, ring_stride, col0, c, sl, st_w[q]);
     return;
@@ -306,6 +310,13 @@ __device__ __forceinline__ void cell_apply(const int* tab, const int* link, cons
     apply_one<GLOBAL_RING>(ring, ring_stride, col0, c, sl, st_w[(int)(best & 1023)]);
     last = best;
   }
+}
+
+template <bool GLOBAL_RING, bool KEYED, int TS>
+__device__ __forceinline__ void cell_apply(const int* tab, const int* link, const int* okey,
+                                           const float* st_w, unsigned h, int q, int c, int sl,
+                                           float* ring, int ring_stride, int col0) {
+  cell_apply_list<GLOBAL_RING, KEYED>(tab[TS + h], link, okey, st_w, q, c, sl, ring, ring_stride, col0);
 }
 
 template <bool GLOBAL_RING>
@@ -481,8 +492,15 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
   // SORT with a.s_table: the per-cell table for whole chunks (kSTable keys,
   // kSTable list heads, CH links)
   int* ctab = reinterpret_cast<int*>(EP ? psi + nc : tr);
-  if (MODE == MODE_SORT && a.s_table)
+  // s_table 2: bitmaps of the ring's cells after the table's links, two
+  // pairs (seen, more than once) used by alternate chunks
+  const int nbw = (int)(((size_t)R * nc + 31) / 32);
+  unsigned* cbits = reinterpret_cast<unsigned*>(ctab + 2 * kSTable + CH);
+  if (MODE == MODE_SORT && a.s_table) {
     for (int i = tid; i < 2 * kSTable; i += nthr) ctab[i] = 0;  // ordered by the loop's first barrier
+    if (a.s_table == 2)
+      for (int i = tid; i < 4 * nbw; i += nthr) cbits[i] = 0u;
+  }
 
   for (;;) {
     if (tid == 0) s_q = (int)atomicAdd(&a.ctl[1], 1u);
@@ -625,6 +643,59 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
             return a.edges[fired[k] + (e - pref[k])];
           };
           uint2 ed_next = q < E ? edge_of(q) : make_uint2(0u, 0u);
+          if (a.s_table == 2) {
+            // Only cells hit more than once in a chunk need the table: every
+            // event marks its cell in the chunk's bitmap pair (a second mark
+            // sets the "more than once" bit); after one barrier a cell hit
+            // once takes its event directly and the others go through the
+            // table, applied after a second barrier.  Each event clears its
+            // cell's words once it has read them; the pairs alternate, so a
+            // chunk's marks never meet the previous chunk's clears.  (A
+            // shared-memory atomic add for the single events and bulk clears
+            // of the idle pair both measured slower.)
+            int pair = 0;
+            for (int e0 = 0; e0 < E; e0 += CH, pair ^= 1) {
+              const int ce = min(CH, E - e0);
+              const uint2 ed = ed_next;
+              unsigned* seen = cbits + (size_t)pair * 2 * nbw;
+              unsigned* more = seen + nbw;
+              int c = 0, sl = 0, bw = 0;
+              unsigned bm = 0, h = 0;
+              float w = 0.f;
+              if (q < ce) {
+                sl = ring_slot(s0, edge_delay(ed), R);
+                c = edge_col(ed);
+                w = edge_w(ed);
+                const int bit = sl * nc + c;
+                bw = bit >> 5;
+                bm = 1u << (bit & 31);
+                if (atomicOr(&seen[bw], bm) & bm) atomicOr(&more[bw], bm);
+              }
+              __syncthreads();
+              if (e0 + CH + q < E) ed_next = edge_of(e0 + CH + q);
+              bool first = false;
+              if (q < ce) {
+                if (!(more[bw] & bm)) {
+                  apply_one<false>(ring, nc, 0, c, sl, w);
+                } else {
+                  st_w[q] = w;
+                  h = cell_insert<kSTable>(ctab, ctab + 2 * kSTable, q, c, sl, &first);
+                }
+              }
+              __syncthreads();
+              if (q < ce) {
+                seen[bw] = 0u;
+                more[bw] = 0u;
+              }
+              if (first) {
+                cell_apply<false, false, kSTable>(ctab, ctab + 2 * kSTable, nullptr, st_w, h, q, c, sl, ring,
+                                                  nc, 0);
+                ctab[h] = 0;
+                ctab[kSTable + h] = 0;
+              }
+            }
+            __syncthreads();
+          } else
           for (int e0 = 0; e0 < E; e0 += CH) {
             const int ce = min(CH, E - e0);
             const uint2 ed = ed_next;
@@ -1443,21 +1514,25 @@ static int launch_tier_s_kernel(const Graph* g, int B, const FwdArgs& a_in, cuda
   SNCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tier_s<MODE, EP>, nthr, smem));
   a.s_table = 0;
   if (MODE == MODE_SORT) {
-    // the per-cell table when it fits without costing a CTA per SM
-    const size_t smem_t = tier_s_bytes(g->N, g->ncols, g->R, a.noc, MODE, EP, nthr, true);
-    int per_sm_t = 0;
-    if ((int)smem_t <= optin_smem() &&
-        cudaFuncSetAttribute(k_tier_s<MODE, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t) ==
-            cudaSuccess &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, k_tier_s<MODE, EP>, nthr, smem_t) ==
-            cudaSuccess &&
-        per_sm_t >= per_sm && per_sm_t >= 1) {
-      smem = smem_t;
-      a.s_table = 1;
-    } else {
-      cudaGetLastError();
-      SNCB_CUDA(cudaFuncSetAttribute(k_tier_s<MODE, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // the per-cell table (and the cell bitmaps with it) when it fits without
+    // costing a CTA per SM; the richest layout that fits
+    for (int tab = 2; tab >= 1 && !a.s_table; --tab) {
+      const size_t smem_t = tier_s_bytes(g->N, g->ncols, g->R, a.noc, MODE, EP, nthr, tab);
+      int per_sm_t = 0;
+      if ((int)smem_t <= optin_smem() &&
+          cudaFuncSetAttribute(k_tier_s<MODE, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t) ==
+              cudaSuccess &&
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, k_tier_s<MODE, EP>, nthr, smem_t) ==
+              cudaSuccess &&
+          per_sm_t >= per_sm && per_sm_t >= 1) {
+        smem = smem_t;
+        a.s_table = tab;
+      } else {
+        cudaGetLastError();
+      }
     }
+    if (!a.s_table)
+      SNCB_CUDA(cudaFuncSetAttribute(k_tier_s<MODE, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   }
   if (per_sm < 1) {
     set_error("tier S does not fit on an SM");
@@ -1512,8 +1587,34 @@ struct GPlan {
 // want_rsm: -1 automatic (shared-memory ring slices when one sample fits),
 // 0 global ring, 1 shared-memory slices (rsm false in the result when they do
 // not fit); want_wave: 0 automatic (as many samples as fit), else at most that.
+// Static shared memory of the tier-G kernels (the largest instance): the
+// dynamic allocation may use what the opt-in limit leaves beside it.
+static size_t tier_g_static_smem() {
+  static size_t cached = 0;
+  static bool done = false;
+  if (!done) {
+    const void* fns[] = {(const void*)k_tier_g<MODE_ATOMIC, false, false>,
+                         (const void*)k_tier_g<MODE_BUCKET, true, false>,
+                         (const void*)k_tier_g<MODE_BUCKET, false, false>,
+                         (const void*)k_tier_g<MODE_SORT, true, false>,
+                         (const void*)k_tier_g<MODE_SORT, false, false>,
+                         (const void*)k_tier_g<MODE_ATOMIC, false, true>,
+                         (const void*)k_tier_g<MODE_SORT, true, true>,
+                         (const void*)k_tier_g<MODE_SORT, false, true>};
+    size_t m = 0;
+    for (const void* f : fns) {
+      cudaFuncAttributes fa{};
+      if (cudaFuncGetAttributes(&fa, f) == cudaSuccess) m = std::max(m, fa.sharedSizeBytes);
+      else cudaGetLastError();
+    }
+    cached = m;
+    done = true;
+  }
+  return cached;
+}
+
 static GPlan plan_tier_g(const Graph* g, int B, int mode, int want_rsm = -1, int want_wave = 0) {
-  const size_t optin = (size_t)optin_smem();
+  const size_t optin = (size_t)optin_smem() - std::min((size_t)optin_smem(), tier_g_static_smem());
   GPlan p{false, 1, 0};
   int cap = std::max(1, std::min(B, kMaxWave));
   if (want_wave > 0) cap = std::min(cap, want_wave);
