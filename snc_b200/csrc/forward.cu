@@ -649,7 +649,8 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
             // sets the "more than once" bit); after one barrier a cell hit
             // once takes its event directly and the others go through the
             // table, applied after a second barrier.  Each event clears its
-            // cell's words once it has read them; the pairs alternate, so a
+            // cell's seen word once it has read it (the events of shared cells
+            // also their "more" word); the pairs alternate, so a
             // chunk's marks never meet the previous chunk's clears.  (A
             // shared-memory atomic add for the single events and bulk clears
             // of the idle pair both measured slower.)
@@ -673,9 +674,10 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
               }
               __syncthreads();
               if (e0 + CH + q < E) ed_next = edge_of(e0 + CH + q);
-              bool first = false;
+              bool first = false, shared_cell = false;
               if (q < ce) {
-                if (!(more[bw] & bm)) {
+                shared_cell = (more[bw] & bm) != 0u;
+                if (!shared_cell) {
                   apply_one<false>(ring, nc, 0, c, sl, w);
                 } else {
                   st_w[q] = w;
@@ -685,7 +687,7 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
               __syncthreads();
               if (q < ce) {
                 seen[bw] = 0u;
-                more[bw] = 0u;
+                if (shared_cell) more[bw] = 0u;  // other words of `more` stayed zero
               }
               if (first) {
                 cell_apply<false, false, kSTable>(ctab, ctab + 2 * kSTable, nullptr, st_w, h, q, c, sl, ring,
