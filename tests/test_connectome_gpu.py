@@ -114,3 +114,46 @@ def test_cotrain_rounds_keep_the_budget():
         S = S - r["pruned"] + r["grown"]
         assert r["synapses"] == S
     assert con.num_synapses() == S == con.host_graph().num_synapses
+
+
+def test_prune_at_scale_removes_exactly_the_weakest():
+    """Two million synapses, 50 000 pruned: the device removes exactly the K
+    smallest (|w|, position) keys (the radix select's eight passes), keeps
+    every other edge in its row order with its weight and age advanced,
+    appends each grown edge after its pre's kept edges, grows only from the
+    previous layer and never duplicates a pair."""
+    layers = [20000, 8000, 100]
+    dev = ST.DeviceConnectome.layered_local(layers, 2_000_000, 1, 0.05, 9)
+    rng = np.random.default_rng(4)
+    S = dev.num_synapses()
+    w = rng.normal(0, 0.3, S).astype(np.float32)
+    w[rng.random(S) < 0.01] = 0.0  # ties of |w| broken by position
+    dev.set_edge_weights(w)
+    row_ptr, post, delay, w0, age0 = dev.to_csr()
+    K = 50_000
+    order = np.lexsort((np.arange(S), np.abs(w0)))
+    pruned = np.zeros(S, bool)
+    pruned[order[:K]] = True
+    fires = rng.integers(0, 50, sum(layers)).astype(np.int64)
+    rep = dev.structural_update(fires, ST.StructConfig(grow_per_epoch=K, protect_rounds=0, delay=2))
+    assert rep[0] == K and 0 < rep[1] <= K and rep[2] == S - K + rep[1]
+    rp2, post2, delay2, w2, age2 = dev.to_csr()
+    n = sum(layers)
+    grown_pairs = set()
+    layer_of = np.repeat(np.arange(len(layers)), layers)
+    for q in range(n):
+        a, b = row_ptr[q], row_ptr[q + 1]
+        keep = ~pruned[a:b]
+        a2, b2 = rp2[q], rp2[q + 1]
+        k = int(keep.sum())
+        np.testing.assert_array_equal(post2[a2:a2 + k], post[a:b][keep])
+        np.testing.assert_array_equal(w2[a2:a2 + k].view(np.uint32), w0[a:b][keep].view(np.uint32))
+        np.testing.assert_array_equal(age2[a2:a2 + k], np.minimum(age0[a:b][keep] + (age0[a:b][keep] < (1 << 20)),
+                                                                  1 << 20))
+        g = post2[a2 + k:b2]
+        assert np.all(delay2[a2 + k:b2] == 2) and np.all(age2[a2 + k:b2] == 1)
+        assert len(set(post2[a2:b2].tolist())) == b2 - a2  # no duplicate pair in the row
+        for p in g.tolist():
+            assert layer_of[p] == layer_of[q] + 1
+            grown_pairs.add((q, p))
+    assert len(grown_pairs) == rep[1]
