@@ -672,8 +672,10 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
                 bm = 1u << (bit & 31);
                 if (atomicOr(&seen[bw], bm) & bm) atomicOr(&more[bw], bm);
               }
-              __syncthreads();
+              // the next chunk's edge: its row search overlaps the marks and
+              // the barrier, its load the apply
               if (e0 + CH + q < E) ed_next = edge_of(e0 + CH + q);
+              __syncthreads();
               bool first = false, shared_cell = false;
               if (q < ce) {
                 shared_cell = (more[bw] & bm) != 0u;
