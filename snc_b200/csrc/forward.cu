@@ -527,10 +527,31 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
     uint32_t* rast = a.raster ? a.raster + a.raster_off[b] : nullptr;
     long long my_spikes = 0, my_events = 0;
     int s0 = 0;
+    __shared__ int s_bc[2][32];  // ballot_compact_1 buffers, alternated
+    int bcp = 0;
+    // the drive of step t: thread i holds entry i of the step's schedule in
+    // registers, loaded a step ahead (entries beyond blockDim.x are read in
+    // the step itself); a step's entries name distinct neurons
+    int pf_lo = T > 0 ? sp[0] : 0, pf_hi = T > 0 ? sp[1] : 0, pf_nid = -1;
+    float pf_ext = 0.f;
+    if (pf_lo + tid < pf_hi) {
+      pf_nid = a.sched_nid[pf_lo + tid];
+      pf_ext = a.sched_ext[pf_lo + tid];
+    }
     for (int t = 0; t < T; ++t) {
       float* slot = ring + (size_t)s0 * nc;
-      for (int k = sp[t] + tid; k < sp[t + 1]; k += nthr) ext[a.sched_nid[k]] = a.sched_ext[k];
+      if (pf_nid >= 0) ext[pf_nid] = pf_ext;
+      for (int k = pf_lo + nthr + tid; k < pf_hi; k += nthr) ext[a.sched_nid[k]] = a.sched_ext[k];
       __syncthreads();
+      pf_nid = -1;
+      if (t + 1 < T) {
+        pf_lo = sp[t + 1];
+        pf_hi = sp[t + 2];
+        if (pf_lo + tid < pf_hi) {
+          pf_nid = a.sched_nid[pf_lo + tid];
+          pf_ext = a.sched_ext[pf_lo + tid];
+        }
+      }
       // integrate / fire, ascending fired list via ballot compaction
       int nf = 0;
       for (int base = 0; base < N; base += nthr) {
@@ -574,7 +595,8 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
         }
         int tot;
         unsigned m;
-        const int pos = ballot_compact(f, scratch, &tot, &m);
+        const int pos = ballot_compact_1(f, s_bc[bcp], &tot, &m);
+        bcp ^= 1;
         if (rast && lane == 0 && base + warp * 32 < N)
           rast[(size_t)t * a.W + ((base + warp * 32) >> 5)] = m;
         if (f) fired[nf + pos] = j;
@@ -698,7 +720,7 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
                 ctab[kSTable + h] = 0;
               }
             }
-            __syncthreads();
+            // the step's closing barrier orders the last chunk's apply
           } else
           for (int e0 = 0; e0 < E; e0 += CH) {
             const int ce = min(CH, E - e0);
