@@ -100,6 +100,7 @@ struct FwdArgs {
   unsigned long long* fires;
   float gamma, trace_decay;
   int s_table;  // tier S SORT: 1 the whole-chunk cell table, 2 also the cell bitmaps
+  int s_lean;   // tier S SORT with the table: the column-list arrays left out
   // deferred eligibility: psi of every ring column and step, [B][ncols][psi_T]
   // (null: eligibility accumulated in the forward into elig)
   float* psi_hist;
@@ -136,9 +137,12 @@ constexpr int kSTable = 2048;
 static size_t cell_bitmap_words(int ncols, int R) { return ((size_t)R * ncols + 31) / 32; }
 
 static size_t tier_s_bytes(int N, int ncols, int R, int noc, int mode, bool eprop, int nthr,
-                           int table = 0) {
+                           int table = 0, bool lean = false) {
   size_t words = (size_t)R * ncols + 4 * (size_t)N + (size_t)noc;
-  if (mode == MODE_SORT) words += (size_t)N + 1 + 2 * (size_t)ncols + 4 * (size_t)nthr;
+  // SORT: row prefix, then the column-list arrays (head, tail, staged column,
+  // slot, weight, link) or, lean, the staged weights alone
+  if (mode == MODE_SORT)
+    words += (size_t)N + 1 + (table && lean ? (size_t)nthr : 2 * (size_t)ncols + 4 * (size_t)nthr);
   if (eprop) words += (size_t)N + ncols;
   if (mode == MODE_SORT && table) words += 2 * (size_t)kSTable + nthr;
   if (mode == MODE_SORT && table == 2) words += 4 * cell_bitmap_words(ncols, R);
@@ -479,14 +483,18 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
   int* fired = reinterpret_cast<int*>(ext + N);
   int* counts = fired + N;
   int* pref = counts + noc;
+  // the column-list apply's arrays (SORT without the cell table); the lean
+  // table layout of the e-prop kernel keeps only the staged weights of them
+  // (the forward keeps the fixed layout, measured faster)
+  const bool lists = MODE == MODE_SORT && !(EP && a.s_lean);
   int* head = pref + (N + 1);
-  int* tail = head + nc;
-  int* st_col = tail + nc;
-  int* st_slot = st_col + CH;
-  float* st_w = reinterpret_cast<float*>(st_slot + CH);
+  int* tail = head + (lists ? nc : 0);
+  int* st_col = tail + (lists ? nc : 0);
+  int* st_slot = st_col + (lists ? CH : 0);
+  float* st_w = reinterpret_cast<float*>(st_slot + (lists ? CH : 0));
   int* st_next = reinterpret_cast<int*>(st_w + CH);
   // e-prop: pre-synaptic trace per neuron, surrogate psi per ring column
-  float* tr = MODE == MODE_SORT ? reinterpret_cast<float*>(st_next + CH)
+  float* tr = MODE == MODE_SORT ? reinterpret_cast<float*>(st_next + (lists ? CH : 0))
                                 : reinterpret_cast<float*>(counts + noc);
   float* psi = tr + N;
   // SORT with a.s_table: the per-cell table for whole chunks (kSTable keys,
@@ -517,7 +525,7 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
       if (EP) tr[i] = 0.f;
     }
     for (int i = tid; i < noc; i += nthr) counts[i] = 0;
-    if (MODE == MODE_SORT)
+    if (lists)
       for (int i = tid; i < nc; i += nthr) {
         head[i] = -1;
         tail[i] = -1;
@@ -1539,11 +1547,16 @@ static int launch_tier_s_kernel(const Graph* g, int B, const FwdArgs& a_in, cuda
   int per_sm = 0;
   SNCB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tier_s<MODE, EP>, nthr, smem));
   a.s_table = 0;
+  a.s_lean = 0;
   if (MODE == MODE_SORT) {
     // the per-cell table (and the cell bitmaps with it) when it fits without
-    // costing a CTA per SM; the richest layout that fits
-    for (int tab = 2; tab >= 1 && !a.s_table; --tab) {
-      const size_t smem_t = tier_s_bytes(g->N, g->ncols, g->R, a.noc, MODE, EP, nthr, tab);
+    // costing a CTA per SM; the richest layout that fits, the full one before
+    // the lean one (e-prop only)
+    for (int v = 0; v < 4 && !a.s_table; ++v) {
+      const int tab = 2 - v / 2;
+      const bool lean = (v & 1) != 0;
+      if (lean && !EP) continue;
+      const size_t smem_t = tier_s_bytes(g->N, g->ncols, g->R, a.noc, MODE, EP, nthr, tab, lean);
       int per_sm_t = 0;
       if ((int)smem_t <= optin_smem() &&
           cudaFuncSetAttribute(k_tier_s<MODE, EP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t) ==
@@ -1553,6 +1566,7 @@ static int launch_tier_s_kernel(const Graph* g, int B, const FwdArgs& a_in, cuda
           per_sm_t >= per_sm && per_sm_t >= 1) {
         smem = smem_t;
         a.s_table = tab;
+        a.s_lean = lean ? 1 : 0;
       } else {
         cudaGetLastError();
       }
