@@ -41,8 +41,15 @@ struct snc_b200_eprop {
   int last_B = 0;
   bool have_elig = false;
   // deferred eligibility: the forward records psi per ring column and step
-  // and the spike raster; k_elig_deferred then builds E from them
-  sncb::DevBuf psi_hist, raster;
+  // and the spike raster; k_raster_t and k_elig_col then build E from them
+  sncb::DevBuf psi_hist, raster, raster_t;
+  // incoming synapses of every ring column: (edge, pre) pairs grouped by
+  // column (cin[cptr[c] .. cptr[c+1])), and the prefix of their 32-synapse
+  // groups (gptr) -- the deferred eligibility's work items
+  int* cptr = nullptr;            // [ncols + 1]
+  int2* cin = nullptr;            // [S]
+  int* gptr = nullptr;            // [ncols + 1]
+  int n_groups = 0;
   // grid mode: one sample's state does not fit one CTA's shared memory, so
   // the forward runs on the all-SM kernel, which reads destination-grouped
   // edges: a grouped copy of the trainer's weights, kept in step with them
@@ -136,57 +143,70 @@ static int sync_gedges(snc_b200_eprop* s, cudaStream_t st) {
 // Most bytes the psi history of one minibatch may take; beyond it the
 // eligibility is accumulated inside the forward instead.
 constexpr size_t kPsiHistMax = size_t(2) << 30;
-constexpr int kEligPerLane = 4;  // synapses of one row held per lane
+
+// The spike raster ([t][word] bits, raster_off per sample) transposed to
+// one run of time bits per neuron: rt[b][i][w] bit u = fired_i(32 w + u)
+// (zero from step T_b on).  A warp per (sample, 32 steps, 32 neurons): each
+// lane reads one step's word and 32 ballots turn the 32 x 32 bit tile.
+__global__ void k_raster_t(int B, int N, int W, int TW, const int* steps, const long long* raster_off,
+                           const uint32_t* raster, uint32_t* rt) {
+  const int lane = threadIdx.x & 31;
+  const long long tiles = (long long)B * TW * W;
+  for (long long wi = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); wi < tiles;
+       wi += (long long)gridDim.x * (blockDim.x >> 5)) {
+    const int b = (int)(wi / ((long long)TW * W));
+    const int r = (int)(wi - (long long)b * TW * W);
+    const int wt = r / W, wn = r - wt * W;
+    const int t = 32 * wt + lane;
+    const uint32_t word = t < steps[b] ? raster[raster_off[b] + (size_t)t * W + wn] : 0u;
+    uint32_t mine = 0;
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+      const uint32_t m = __ballot_sync(0xffffffffu, (word >> k) & 1u);
+      if (lane == k) mine = m;
+    }
+    const int i = 32 * wn + lane;
+    if (i < N) rt[((size_t)b * N + i) * TW + wt] = mine;
+  }
+}
 
 // Eligibility of every synapse after the forward of a minibatch
 // (cuda_trainer.cu:105-112 restated per synapse): for sample b and synapse e
 // (pre i, post column c), E[b][e] = sum over t = 0..T_b-1, in step order, of
-// psi[b][c][t] * tr_i(t), with the pre trace rebuilt from the raster,
+// psi[b][c][t] * tr_i(t), with the pre trace rebuilt from the spikes,
 // tr_i(t) = decay * tr_i(t-1) + (1 - decay) * fired_i(t), and every product
 // and sum rounded as the per-step update rounds it; steps whose trace is
-// exactly zero add nothing (trainer.cpp:243-244).  One warp per (sample,
-// row); each lane keeps kEligPerLane synapses of the row in registers.
-__global__ void k_elig_deferred(int B, int N, int S, const int* row_ptr, const uint2* edges,
-                                const int* steps, const long long* raster_off,
-                                const uint32_t* raster, int W, const float* psi, int nc, int psi_T,
-                                float decay, float* elig) {
+// exactly zero add nothing (trainer.cpp:243-244).  One warp per (sample, 32
+// incoming synapses of one column): the column's psi history is read once
+// per 32 steps (one coalesced load, then broadcast by shuffles) and each
+// lane's pre spikes come 32 steps to a word from the transposed raster.
+__global__ void k_elig_col(int B, int N, int S, int nc, int G, const int* cptr, const int2* cin,
+                           const int* gptr, const int* steps, const uint32_t* rt, int TW,
+                           const float* psi, int psi_T, float decay, float* elig) {
   const int lane = threadIdx.x & 31;
-  const long long nwarps_total = (long long)gridDim.x * (blockDim.x >> 5);
   const float c1 = __fsub_rn(1.f, decay);
   for (long long wi = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-       wi < (long long)B * N; wi += nwarps_total) {
-    const int b = (int)(wi / N), i = (int)(wi - (long long)b * N);
-    const int rs = row_ptr[i], re = row_ptr[i + 1];
-    if (rs == re) continue;
+       wi < (long long)B * G; wi += (long long)gridDim.x * (blockDim.x >> 5)) {
+    const int b = (int)(wi / G), gi = (int)(wi - (long long)b * G);
+    const int c = upper_index(gptr, nc, gi);
+    const int idx = cptr[c] + 32 * (gi - gptr[c]) + lane;
+    const bool valid = idx < cptr[c + 1];
+    const int2 ep = valid ? cin[idx] : make_int2(0, 0);
     const int T = steps[b];
-    const uint32_t* rw = raster + raster_off[b] + (i >> 5);
-    const uint32_t bit = 1u << (i & 31);
-    const float* pb = psi + (size_t)b * nc * psi_T;
-    float* Eb = elig + (size_t)b * S;
-    for (int e0 = rs; e0 < re; e0 += 32 * kEligPerLane) {
-      const float* prow[kEligPerLane];
-      float acc[kEligPerLane];
-#pragma unroll
-      for (int k = 0; k < kEligPerLane; ++k) {
-        const int e = e0 + lane + 32 * k;
-        prow[k] = e < re ? pb + (size_t)edge_col(edges[e]) * psi_T : nullptr;
-        acc[k] = 0.f;
-      }
-      float tr = 0.f;
-      for (int t = 0; t < T; ++t) {
-        const float f = (__ldg(rw + (size_t)t * W) & bit) ? 1.f : 0.f;
-        tr = __fadd_rn(__fmul_rn(decay, tr), __fmul_rn(c1, f));
-        if (tr == 0.f) continue;
-#pragma unroll
-        for (int k = 0; k < kEligPerLane; ++k)
-          if (prow[k]) acc[k] = __fadd_rn(acc[k], __fmul_rn(__ldg(prow[k] + t), tr));
-      }
-#pragma unroll
-      for (int k = 0; k < kEligPerLane; ++k) {
-        const int e = e0 + lane + 32 * k;
-        if (e < re) Eb[e] = acc[k];
+    const float* pc = psi + ((size_t)b * nc + c) * psi_T;
+    const uint32_t* rw = rt + ((size_t)b * N + ep.y) * TW;
+    float acc = 0.f, tr = 0.f;
+    for (int t0 = 0; t0 < T; t0 += 32) {
+      const float pv = t0 + lane < T ? pc[t0 + lane] : 0.f;
+      const uint32_t word = valid ? rw[t0 >> 5] : 0u;
+      const int n = min(32, T - t0);
+      for (int u = 0; u < n; ++u) {
+        const float p = __shfl_sync(0xffffffffu, pv, u);
+        tr = __fadd_rn(__fmul_rn(decay, tr), __fmul_rn(c1, (word >> u) & 1u ? 1.f : 0.f));
+        if (tr != 0.f) acc = __fadd_rn(acc, __fmul_rn(p, tr));
       }
     }
+    if (valid) elig[(size_t)b * S + ep.x] = acc;
   }
 }
 
@@ -200,6 +220,10 @@ static void free_session(snc_b200_eprop* s) {
   if (s->ev1) cudaEventDestroy(s->ev1);
   s->psi_hist.release();
   s->raster.release();
+  s->raster_t.release();
+  dev_free(s->cptr);
+  dev_free(s->cin);
+  dev_free(s->gptr);
   if (s->run) {
     // the run borrows the session's outputs and control words
     s->run->counts = nullptr;
@@ -236,6 +260,25 @@ static int create_session(snc_b200_eprop* s, const Graph* g, const snc_lif* lif,
   for (int e = 0; e < S; ++e) std::memcpy(&edges[e].y, &w[e], 4);
   int rc;
   if ((rc = dev_upload(&s->edges, edges.data(), edges.size()))) return rc;
+  {
+    // incoming synapses per ring column, for the deferred eligibility
+    const int nc = std::max(1, g->ncols);
+    std::vector<int> cptr(nc + 1, 0), gptr(nc + 1, 0);
+    for (int e = 0; e < S; ++e) cptr[(edges[e].x & 0xFFFFFFu) + 1]++;
+    for (int c = 0; c < nc; ++c) {
+      gptr[c + 1] = gptr[c] + (cptr[c + 1] + 31) / 32;
+      cptr[c + 1] += cptr[c];
+    }
+    std::vector<int2> cin((size_t)std::max(1, S));
+    std::vector<int> fill(cptr.begin(), cptr.end() - 1);
+    for (int i = 0; i < N; ++i)
+      for (int e = g->row_ptr_h[i]; e < g->row_ptr_h[i + 1]; ++e)
+        cin[fill[edges[e].x & 0xFFFFFFu]++] = make_int2(e, i);
+    s->n_groups = gptr[nc];
+    if ((rc = dev_upload(&s->cptr, cptr.data(), cptr.size()))) return rc;
+    if ((rc = dev_upload(&s->gptr, gptr.data(), gptr.size()))) return rc;
+    if ((rc = dev_upload(&s->cin, cin.data(), cin.size()))) return rc;
+  }
   if ((rc = dev_upload(&s->bmat, feedback, (size_t)std::max(1, s->n_internal) * s->oc))) return rc;
   if ((rc = dev_upload(&s->internal_row, irow.data(), (size_t)N))) return rc;
   const size_t B = (size_t)max_batch;
@@ -356,6 +399,11 @@ static int run_batch(snc_b200_eprop* s, const snc_input_event* ev, size_t n_ev, 
       free_inputs(&in);
       return rc;
     }
+    const size_t tw = ((size_t)std::max(1, in.Tmax) + 31) / 32;
+    if ((rc = s->raster_t.reserve((size_t)B * std::max(1, N) * tw * sizeof(uint32_t)))) {
+      free_inputs(&in);
+      return rc;
+    }
   }
   if (train && !deferred) chk(cudaMemsetAsync(s->elig, 0, (size_t)B * S * sizeof(float), st), "memset elig");
   if (train) {
@@ -408,13 +456,16 @@ static int run_batch(snc_b200_eprop* s, const snc_input_event* ev, size_t n_ev, 
       int dev = 0, sms = 148;
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      const long long warps = (long long)B * N;
-      const int blocks = (int)std::max(1ll, std::min((warps + 7) / 8, (long long)sms * 8));
-      k_elig_deferred<<<blocks, 256, 0, st>>>(B, N, S, g->row_ptr, s->edges, in.steps, in.raster_off,
-                                              static_cast<const uint32_t*>(s->raster.p), W,
-                                              static_cast<const float*>(s->psi_hist.p),
-                                              std::max(1, g->ncols), std::max(1, in.Tmax),
-                                              s->cfg.trace_decay, s->elig);
+      const int TW = (std::max(1, in.Tmax) + 31) / 32;
+      uint32_t* rt = static_cast<uint32_t*>(s->raster_t.p);
+      const long long tiles = (long long)B * TW * W;
+      k_raster_t<<<(int)std::max(1ll, std::min((tiles + 7) / 8, (long long)sms * 8)), 256, 0, st>>>(
+          B, N, W, TW, in.steps, in.raster_off, static_cast<const uint32_t*>(s->raster.p), rt);
+      const long long warps = (long long)B * s->n_groups;
+      if (warps > 0)
+        k_elig_col<<<(int)std::max(1ll, std::min((warps + 7) / 8, (long long)sms * 16)), 256, 0, st>>>(
+            B, N, S, std::max(1, g->ncols), s->n_groups, s->cptr, s->cin, s->gptr, in.steps, rt, TW,
+            static_cast<const float*>(s->psi_hist.p), std::max(1, in.Tmax), s->cfg.trace_decay, s->elig);
       chk(cudaGetLastError(), "deferred eligibility");
     }
   }
