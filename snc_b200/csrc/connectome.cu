@@ -631,6 +631,7 @@ extern "C" int snc_b200_connectome_update(snc_b200_connectome* c, const int64_t*
   }
   // 4. fallback growth onto under-driven posts (random draws)
   int attempts = 0;
+  std::mt19937_64 rng_next = c->rng;
   if ((int)grown.size() < pruned && max_attempts > 0) {
     const int lo = c->layer_begin.size() > 1 ? c->layer_begin[1] : 0, hi = std::max(0, n - 1);
     std::vector<int> draws(4 * (size_t)max_attempts);
@@ -650,9 +651,10 @@ extern "C" int snc_b200_connectome_update(snc_b200_connectome* c, const int64_t*
     attempts = res[0];
     grown.resize(res[1]);
     if (res[1]) SNCB_CUDA(cudaMemcpy(grown.data(), d_grown, 8 * (size_t)res[1], cudaMemcpyDeviceToHost));
-    // the reference's generator advances by exactly the draws consumed
+    // the reference's generator advances by exactly the draws consumed (kept
+    // aside until the new CSR is in place)
     std::uniform_int_distribution<int> any_post(lo, hi);
-    for (long long i = 0; i < 4ll * attempts; ++i) (void)any_post(c->rng);
+    for (long long i = 0; i < 4ll * attempts; ++i) (void)any_post(rng_next);
   }
   // 5. the new CSR
   const int Gn = (int)grown.size();
@@ -715,6 +717,7 @@ extern "C" int snc_b200_connectome_update(snc_b200_connectome* c, const int64_t*
   c->age = age2;
   c->cap = cap2;
   c->S = S2;
+  c->rng = rng_next;
   if (Gn) c->max_delay = std::max(c->max_delay, cfg->delay);
   out->pruned = pruned;
   out->grown = Gn;
