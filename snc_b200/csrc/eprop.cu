@@ -173,12 +173,14 @@ __global__ void k_raster_t(int B, int N, int W, int TW, const int* steps, const 
 // Eligibility of every synapse after the forward of a minibatch
 // (cuda_trainer.cu:105-112 restated per synapse): for sample b and synapse e
 // (pre i, post column c), E[b][e] = sum over t = 0..T_b-1, in step order, of
-// psi[b][c][t] * tr_i(t), with the pre trace rebuilt from the spikes,
+// psi[b][t][c] * tr_i(t), with the pre trace rebuilt from the spikes,
 // tr_i(t) = decay * tr_i(t-1) + (1 - decay) * fired_i(t), and every product
 // and sum rounded as the per-step update rounds it; steps whose trace is
 // exactly zero add nothing (trainer.cpp:243-244).  One warp per (sample, 32
 // incoming synapses of one column): the column's psi history is read once
-// per 32 steps (one coalesced load, then broadcast by shuffles) and each
+// per 32 steps (one gather of 32 steps, then broadcast by shuffles; the
+// history is step-major so that the forward writes each step's values for
+// all columns contiguously) and each
 // lane's pre spikes come 32 steps to a word from the transposed raster.
 __global__ void k_elig_col(int B, int N, int S, int nc, int G, const int* cptr, const int2* cin,
                            const int* gptr, const int* steps, const uint32_t* rt, int TW,
@@ -193,11 +195,11 @@ __global__ void k_elig_col(int B, int N, int S, int nc, int G, const int* cptr, 
     const bool valid = idx < cptr[c + 1];
     const int2 ep = valid ? cin[idx] : make_int2(0, 0);
     const int T = steps[b];
-    const float* pc = psi + ((size_t)b * nc + c) * psi_T;
+    const float* pc = psi + (size_t)b * psi_T * nc + c;  // step-major: stride nc
     const uint32_t* rw = rt + ((size_t)b * N + ep.y) * TW;
     float acc = 0.f, tr = 0.f;
     for (int t0 = 0; t0 < T; t0 += 32) {
-      const float pv = t0 + lane < T ? pc[t0 + lane] : 0.f;
+      const float pv = t0 + lane < T ? pc[(size_t)(t0 + lane) * nc] : 0.f;
       const uint32_t word = valid ? rw[t0 >> 5] : 0u;
       const int n = min(32, T - t0);
       for (int u = 0; u < n; ++u) {

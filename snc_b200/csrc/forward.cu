@@ -589,7 +589,7 @@ __global__ void __launch_bounds__(1024, 1) k_tier_s(FwdArgs a) {
             if (c >= 0) {
               const float ps = dd < 1.f ? __fmul_rn(a.gamma, __fsub_rn(1.f, dd)) : 0.f;
               psi[c] = ps;
-              if (a.psi_hist) a.psi_hist[((size_t)b * nc + c) * a.psi_T + t] = ps;
+              if (a.psi_hist) a.psi_hist[((size_t)b * a.psi_T + t) * nc + c] = ps;
             }
             tr[j] = __fadd_rn(__fmul_rn(a.trace_decay, tr[j]),
                               __fmul_rn(__fsub_rn(1.f, a.trace_decay), f ? 1.f : 0.f));
@@ -941,7 +941,7 @@ __device__ void phase_a(const FwdArgs& a, const GSmem& sm, int* scratch, unsigne
         // column and step, for the deferred eligibility
         const float thr = a.lif.thr;
         const float dd = __fdiv_rn(fabsf(__fsub_rn(vpre, thr)), thr > 0.f ? thr : 1.f);
-        a.psi_hist[((size_t)sample * nc + c) * a.psi_T + t] =
+        a.psi_hist[((size_t)sample * a.psi_T + t) * nc + c] =
             dd < 1.f ? __fmul_rn(a.gamma, __fsub_rn(1.f, dd)) : 0.f;
       }
       if (PERSIST) {
