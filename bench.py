@@ -58,7 +58,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--mode", default="auto", choices=["auto", "atomic", "bucket", "sort"])
     p.add_argument("--no-extra", action="store_true", help="skip the plain / sort / cpu legs")
-    p.add_argument("--leg", choices=["bptt", "bptt-custom", "configs", "reference-gpu", "c3"],
+    p.add_argument("--leg", choices=["bptt", "bptt-custom", "configs", "reference-gpu", "c3", "eprop"],
                    help="run only this extra leg on one GPU and print its JSON (for profiling)")
     return p.parse_args()
 
@@ -341,7 +341,20 @@ def config_legs(reps=3):
         di.release()
     out["encode_C3"] = leg
     dg.release()
-    # e-prop: one C3 minibatch
+    out["eprop_C3"] = eprop_leg(lif, reps)
+    return out
+
+
+def eprop_leg(lif=None, reps=3):
+    """One C3 e-prop minibatch (32 samples, the graph's own weights) with
+    SORT and ATOMIC delivery beside the CPU restatement (also `--leg eprop`,
+    for profiling)."""
+    import torch
+    from oracle import oracle as O
+    from snc_b200 import eprop as EP
+    from snc_b200 import runtime as R
+    from snc_b200 import workloads as W
+    lif = lif or W.lif_tau20()
     g = W.audio700_graph()
     ev, steps = W.audio700_inputs(32)
     labels = np.random.default_rng(5).integers(0, g.num_output_channels, 32).astype(np.int32)
@@ -375,15 +388,15 @@ def config_legs(reps=3):
     cpu_ms = 1e3 * (time.perf_counter() - t0)
     diff = float(np.abs(w_gpu - ref["w"]).max() / max(1e-30, float(np.abs(ref["w"]).max())))
     ss = int(np.sum(steps))
-    out["eprop_C3"] = {"batch": 32, "sample_steps": ss, "device_ms": min(dev_ms[1:]),
-                       "wall_ms": min(wall_ms[1:]), "synaptic_events": int(o["events"]),
-                       "events_per_s": o["events"] / (min(dev_ms[1:]) / 1e3),
-                       "device_ms_atomic_delivery": min(atomic_ms[1:]),
-                       "samples_per_s": 32 / (min(wall_ms[1:]) / 1e3),
-                       "cpu_port_ms": cpu_ms, "cpu_cores": 1,
-                       "max_rel_weight_diff": diff}
+    res = {"batch": 32, "sample_steps": ss, "device_ms": min(dev_ms[1:]),
+           "wall_ms": min(wall_ms[1:]), "synaptic_events": int(o["events"]),
+           "events_per_s": o["events"] / (min(dev_ms[1:]) / 1e3),
+           "device_ms_atomic_delivery": min(atomic_ms[1:]),
+           "samples_per_s": 32 / (min(wall_ms[1:]) / 1e3),
+           "cpu_port_ms": cpu_ms, "cpu_cores": 1,
+           "max_rel_weight_diff": diff}
     sess.release()
-    return out
+    return res
 
 
 def graph_build_leg(g, host_build_s):
@@ -879,7 +892,8 @@ def main():
     if args.leg:
         legs = {"bptt": bptt_leg, "bptt-custom": lambda: bptt_leg(with_reference=False),
                 "configs": config_legs, "reference-gpu": reference_gpu_leg,
-                "c3": lambda: c3_leg("atomic" if args.mode == "atomic" else "sort")}
+                "c3": lambda: c3_leg("atomic" if args.mode == "atomic" else "sort"),
+                "eprop": eprop_leg}
         print(json.dumps({args.leg: legs[args.leg]()}), flush=True)
         return 0
     if args.impl == "reference":
