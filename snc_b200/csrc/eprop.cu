@@ -201,11 +201,20 @@ __global__ void k_elig_col(int B, int N, int S, int nc, int G, const int* cptr, 
     for (int t0 = 0; t0 < T; t0 += 32) {
       const float pv = t0 + lane < T ? pc[(size_t)(t0 + lane) * nc] : 0.f;
       const uint32_t word = valid ? rw[t0 >> 5] : 0u;
-      const int n = min(32, T - t0);
-      for (int u = 0; u < n; ++u) {
+      // one step: decay * tr + (1 - decay) * fired, rounded as the per-step
+      // update rounds it (with no spike the second product is +0 and the sum
+      // is decay * tr itself)
+      auto step = [&](int u) {
         const float p = __shfl_sync(0xffffffffu, pv, u);
-        tr = __fadd_rn(__fmul_rn(decay, tr), __fmul_rn(c1, (word >> u) & 1u ? 1.f : 0.f));
+        const float dt = __fmul_rn(decay, tr);
+        tr = (word >> u) & 1u ? __fadd_rn(dt, c1) : dt;
         if (tr != 0.f) acc = __fadd_rn(acc, __fmul_rn(p, tr));
+      };
+      if (T - t0 >= 32) {
+#pragma unroll
+        for (int u = 0; u < 32; ++u) step(u);
+      } else {
+        for (int u = 0; u < T - t0; ++u) step(u);
       }
     }
     if (valid) elig[(size_t)b * S + ep.x] = acc;
