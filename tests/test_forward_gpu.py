@@ -195,6 +195,26 @@ def test_sort_bit_exact_hub_columns(pname, path, force):
 
 
 @pytest.mark.parametrize("pname,path,force", PATHS)
+def test_sort_bit_exact_when_an_inbox_overflows(pname, path, force):
+    # 3000 inputs spread over the grid kernel's blocks all feed the few
+    # hidden neurons of the last block: every step a thousand or more
+    # descriptors reach one inbox, more than it takes, so that block orders
+    # its events from every block's fired list (the scan fallback) while the
+    # others publish their lists after their barrier arrival
+    g = W.random_graph(31, n_in=3000, n_hid=8, n_out=2, p=0.6, max_delay=4, recurrent=False)
+    ev, steps = W.random_events(32, g, 1, [30], rate=0.9)
+    lif = R.LIFParams(threshold=0.5, decay=0.9, reset=0.0, refractory=0, reset_mode=1)
+    ref = O.forward_batched(g, ev, steps, lif)
+    assert int(ref["events"].sum()) > 20000
+    out = run_gpu(g, ev, steps, lif, R.MODE_SORT, path, force_grid=force)
+    assert_exact(out, ref)
+    # the same twice more in one run object: stale fired counts from the
+    # previous launch must not be taken for this one's
+    out2 = run_gpu(g, ev, steps, lif, R.MODE_SORT, path, force_grid=force, repeat=2)
+    assert_exact(out2, ref)
+
+
+@pytest.mark.parametrize("pname,path,force", PATHS)
 def test_graph_without_synapses(pname, path, force):
     # inputs fire from their drive alone; nothing is delivered
     N = 7
