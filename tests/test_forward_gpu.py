@@ -436,3 +436,30 @@ def test_atomic_small_and_uneven_batches(batch):
         assert spike_count_agreement(out["spikes"][b], ref["spikes"][b]) >= 0.99
     agree = np.mean(out["raster"] == ref["raster"])
     assert agree >= 0.99
+
+
+def test_one_call_forward_from_pinned_host_events():
+    """The end-to-end call with its events in pinned host memory (the
+    bench's e2e leg) equals the same call from pageable memory and the CPU
+    backend."""
+    import torch
+    g = W.random_graph(12, n_hid=120, max_delay=7)
+    ev, steps = W.random_events(13, g, 5, [40, 22, 40, 31, 9])
+    lif = R.LIFParams(threshold=1.0, decay=0.9, reset=0.0, refractory=1)
+    ref = O.forward_batched(g, ev, steps, lif)
+    dg = R.DeviceGraph(g)
+    pin = torch.empty(ev.nbytes, dtype=torch.uint8, pin_memory=True)
+    ev_pinned = pin.numpy().view(ev.dtype)
+    ev_pinned[:] = ev
+    a = R.forward_batched(dg, ev_pinned, steps, lif, mode=R.MODE_SORT)
+    b = R.forward_batched(dg, ev, steps, lif, mode=R.MODE_SORT)
+    for k in ("spikes", "events", "logits"):
+        np.testing.assert_array_equal(a[k], b[k])
+        np.testing.assert_array_equal(a[k], ref[k])
+
+
+def test_reduction_rate_probe():
+    """The atomic roofline's denominator: a positive, plausible rate of
+    scattered float reductions (well above a billion per second)."""
+    rate = R.probe_red_rate(1 << 20, 1 << 24)
+    assert 1e9 < rate < 1e13
